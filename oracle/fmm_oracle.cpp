@@ -1,0 +1,1570 @@
+// TEST INFRASTRUCTURE ONLY — the oracle.
+//
+// A plain C++ restatement of the reference FMM's scalar FP64 path
+// (Vedant9500/FMMS, crates/fmm). It exists to check the CUDA engine: only the
+// tests, the smoke check and the CPU-baseline leg of the benchmark may load it.
+// The engine never links or calls it.
+//
+// Operation order follows the reference line by line so that Morton keys, the
+// octree, multipoles, the multipole power, the f pre-pass and therefore the MAC
+// decisions and interaction lists are reproduced bit for bit. Build with
+// -ffp-contract=off: the reference (Rust) never contracts a*b+c into an FMA.
+//
+// Citations are file:line inside crates/fmm/src unless stated otherwise.
+//
+// Parity pinning: the reference is Rust and no Rust toolchain is available, so
+// the reference cannot be run to produce golden outputs. The restatement is
+// pinned against every known-answer test the reference's own test suite holds
+// (tests/test_oracle.py), and the fixtures under tests/golden are generated
+// from it by tests/golden/make_golden.py.
+//
+// Extensions beyond the reference (flagged in every entry point): Plummer
+// softening in P2P and the direct sum, a geometric opening-angle MAC, and a
+// multi-threaded evaluation used only as the timed CPU baseline.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// ---------------------------------------------------------------- complex
+// harmonic.rs:21-74
+struct Cx {
+    double re, im;
+};
+static inline Cx cx(double r, double i) { return Cx{r, i}; }
+static inline Cx cadd(Cx a, Cx b) { return Cx{a.re + b.re, a.im + b.im}; }
+static inline Cx csub(Cx a, Cx b) { return Cx{a.re - b.re, a.im - b.im}; }
+static inline Cx cmul(Cx a, Cx b) {
+    return Cx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+static inline Cx cscale(Cx a, double s) { return Cx{a.re * s, a.im * s}; }
+static inline Cx cconj(Cx a) { return Cx{a.re, -a.im}; }
+static const Cx CZERO = {0.0, 0.0};
+
+static inline size_t dimp(size_t p) { return (p + 1) * (p + 1); }  // harmonic.rs:78
+static inline size_t idx(size_t n, long m) {                      // harmonic.rs:84
+    return (size_t)((long)(n * (n + 1)) + m);
+}
+
+// ---------------------------------------------------------------- models.rs
+// SplitMix64, models.rs:13-31
+struct Rng {
+    uint64_t s;
+    explicit Rng(uint64_t seed) : s(seed) {}
+    uint64_t next_u64() {
+        s += 0x9E3779B97F4A7C15ULL;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    }
+    double unit() { return (double)(next_u64() >> 11) / (double)(1ULL << 53); }
+};
+
+// models.rs:35-58 (Plummer, untruncated, equal masses 1/n)
+static void plummer(size_t n, const double c[3], uint64_t seed, double* mass, double* pos) {
+    Rng rng(seed);
+    const double m = 1.0 / (double)n;
+    for (size_t i = 0; i < n; ++i) {
+        double u = rng.unit();
+        double w = std::pow(u, 2.0 / 3.0);
+        double r = std::sqrt(w / (1.0 - w));
+        double z = 2.0 * rng.unit() - 1.0;
+        double phi = 2.0 * M_PI * rng.unit();
+        double s = std::sqrt(1.0 - z * z);
+        mass[i] = m;
+        pos[3 * i + 0] = c[0] + r * s * std::cos(phi);
+        pos[3 * i + 1] = c[1] + r * s * std::sin(phi);
+        pos[3 * i + 2] = c[2] + r * z;
+    }
+}
+
+// models.rs:61-82 (Hernquist)
+static void hernquist(size_t n, const double c[3], uint64_t seed, double* mass, double* pos) {
+    Rng rng(seed);
+    const double m = 1.0 / (double)n;
+    for (size_t i = 0; i < n; ++i) {
+        double s = std::sqrt(rng.unit());
+        double r = s / (1.0 - s);
+        double z = 2.0 * rng.unit() - 1.0;
+        double phi = 2.0 * M_PI * rng.unit();
+        double sp = std::sqrt(1.0 - z * z);
+        mass[i] = m;
+        pos[3 * i + 0] = c[0] + r * sp * std::cos(phi);
+        pos[3 * i + 1] = c[1] + r * sp * std::sin(phi);
+        pos[3 * i + 2] = c[2] + r * z;
+    }
+}
+
+// ---------------------------------------------------------------- harmonic.rs
+// theta_table_into, harmonic.rs:91-129
+static void theta_table(const double rv[3], size_t p, Cx* t) {
+    const double x = rv[0], y = rv[1], z = rv[2];
+    const double r2 = x * x + y * y + z * z;
+    const double ir = 1.0 / std::sqrt(r2);
+    t[idx(0, 0)] = cx(ir, 0.0);
+    for (size_t n = 1; n <= p; ++n) {
+        double a = (double)(2 * n - 1) * z;
+        double b = (double)((n - 1) * (n - 1));
+        Cx p1 = t[idx(n - 1, 0)];
+        Cx p2 = n >= 2 ? t[idx(n - 2, 0)] : CZERO;
+        t[idx(n, 0)] = cscale(csub(cscale(p1, a), cscale(p2, b)), 1.0 / r2);
+    }
+    for (size_t m = 1; m <= p; ++m) {
+        long mi = (long)m;
+        t[idx(m, mi)] = cmul(cscale(cx(x, y), (double)(2 * m - 1) / r2), t[idx(m - 1, mi - 1)]);
+        for (size_t n = m + 1; n <= p; ++n) {
+            double a = (double)(2 * n - 1) * z;
+            double b = (double)((n - 1) * (n - 1) - m * m);
+            // For n = m+1 the coefficient b is 0 and the reference multiplies a
+            // scratch slot by it; the product is 0 for any finite slot.
+            Cx p2 = (n >= m + 2) ? t[idx(n - 2, mi)] : CZERO;
+            t[idx(n, mi)] = cscale(csub(cscale(t[idx(n - 1, mi)], a), cscale(p2, b)), 1.0 / r2);
+        }
+    }
+    for (size_t m = 1; m <= p; ++m) {
+        double sgn = (m % 2 == 0) ? 1.0 : -1.0;
+        for (size_t n = m; n <= p; ++n)
+            t[idx(n, -(long)m)] = cscale(cconj(t[idx(n, (long)m)]), sgn);
+    }
+}
+
+// upsilon_table_into, harmonic.rs:141-173
+static void upsilon_table(const double rv[3], size_t p, Cx* u) {
+    const double x = rv[0], y = rv[1], z = rv[2];
+    const double r2 = x * x + y * y + z * z;
+    u[idx(0, 0)] = cx(1.0, 0.0);
+    for (size_t m = 0; m <= p; ++m) {
+        long mi = (long)m;
+        if (m > 0) u[idx(m, mi)] = cmul(cscale(cx(x, y), 1.0 / (double)(2 * m)), u[idx(m - 1, mi - 1)]);
+        for (size_t n = m + 1; n <= p; ++n) {
+            double a = (double)(2 * n - 1) * z;
+            double b = r2;
+            double c = (double)(n * n - m * m);
+            Cx p2 = (n >= m + 2) ? u[idx(n - 2, mi)] : CZERO;
+            u[idx(n, mi)] = cscale(csub(cscale(u[idx(n - 1, mi)], a), cscale(p2, b)), 1.0 / c);
+        }
+    }
+    for (size_t m = 1; m <= p; ++m) {
+        double sgn = (m % 2 == 0) ? 1.0 : -1.0;
+        for (size_t n = m; n <= p; ++n)
+            u[idx(n, -(long)m)] = cscale(cconj(u[idx(n, (long)m)]), sgn);
+    }
+}
+
+// ---------------------------------------------------------------- tree.rs
+static const uint32_t BITS = 21;  // tree.rs:16
+
+// tree.rs:28-35
+static uint64_t dilate(uint64_t x) {
+    x &= (1ULL << BITS) - 1;
+    x = (x | (x << 32)) & 0x001f00000000ffffULL;
+    x = (x | (x << 16)) & 0x001f0000ff0000ffULL;
+    x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+    return (x | (x << 2)) & 0x1249249249249249ULL;
+}
+
+// tree.rs:37-46. The quantiser subtracts lo[0] (the x minimum) on every axis.
+static uint64_t quant(double c, double lo0, double inv_side) {
+    double v = (c - lo0) * inv_side;
+    if (v != v) return 0;  // Rust `as u64` maps NaN to 0
+    v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+    return (uint64_t)(v * (double)((1ULL << BITS) - 1));
+}
+static uint64_t morton_key(double x, double y, double z, double lo0, double inv_side) {
+    uint64_t key = dilate(quant(z, lo0, inv_side));
+    key |= dilate(quant(y, lo0, inv_side)) << 1;
+    key |= dilate(quant(x, lo0, inv_side)) << 2;
+    return key;
+}
+
+enum CenterMode { CENTER_COM = 0, CENTER_SPHERE = 1 };
+
+struct Cell {  // tree.rs:49-58
+    size_t first, count;
+    int32_t children[8];
+    bool leaf;
+    uint32_t level;
+    double cen[3];
+    double mass;
+    double rho;
+};
+
+struct Tree {
+    std::vector<Cell> cells;
+    std::vector<uint32_t> order;
+    std::vector<uint64_t> keys_sorted;
+    size_t n_leaf = 16;
+    int mode = CENTER_COM;
+    double lo[3], hi[3], side, inv_side;
+};
+
+static inline double dist2(const double a[3], const double b[3]) {
+    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+static inline double dist(const double a[3], const double b[3]) { return std::sqrt(dist2(a, b)); }
+static inline double fmax_rs(double a, double b) { return std::fmax(a, b); }  // Rust f64::max
+static inline double fmin_rs(double a, double b) { return std::fmin(a, b); }
+
+struct Item {
+    double c[3];
+    double r;
+};
+
+// Ritter grow/enclose sphere, tree.rs:290-389
+static void ritter(const std::vector<Item>& items, double out_c[3], double* out_r) {
+    size_t a = 0, b = 0;
+    double best = -1.0;
+    for (size_t i = 0; i < items.size(); ++i) {
+        double d2 = dist2(items[i].c, items[a].c);
+        if (d2 > best) { best = d2; b = i; }
+    }
+    a = b;
+    best = -1.0;
+    for (size_t i = 0; i < items.size(); ++i) {
+        double d2 = dist2(items[i].c, items[a].c);
+        if (d2 > best) { best = d2; b = i; }
+    }
+    const double* pa = items[a].c;
+    const double* pb = items[b].c;
+    double dir[3];
+    {
+        double dx = pb[0] - pa[0], dy = pb[1] - pa[1], dz = pb[2] - pa[2];
+        double d = fmax_rs(std::sqrt(dx * dx + dy * dy + dz * dz), std::numeric_limits<double>::min());
+        dir[0] = dx / d; dir[1] = dy / d; dir[2] = dz / d;
+    }
+    double far_a[3] = {pa[0] + items[a].r * dir[0], pa[1] + items[a].r * dir[1], pa[2] + items[a].r * dir[2]};
+    double far_b[3] = {pb[0] - items[b].r * dir[0], pb[1] - items[b].r * dir[1], pb[2] - items[b].r * dir[2]};
+    double c[3] = {(far_a[0] + far_b[0]) * 0.5, (far_a[1] + far_b[1]) * 0.5, (far_a[2] + far_b[2]) * 0.5};
+    double r = dist(far_a, far_b) * 0.5;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (const Item& it : items) {
+            double d = dist(it.c, c);
+            if (d + it.r > r) {
+                double dd = fmax_rs(d, std::numeric_limits<double>::min());
+                double dv[3] = {(it.c[0] - c[0]) / dd, (it.c[1] - c[1]) / dd, (it.c[2] - c[2]) / dd};
+                double pp[3] = {it.c[0] + it.r * dv[0], it.c[1] + it.r * dv[1], it.c[2] + it.r * dv[2]};
+                double d_far = d + it.r;
+                double t = (d_far - r) / (2.0 * d_far);
+                for (int k = 0; k < 3; ++k) c[k] += t * (pp[k] - c[k]);
+                r = (d_far + r) * 0.5;
+            }
+        }
+    }
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (const Item& it : items)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin_rs(lo[d], it.c[d] - it.r);
+            hi[d] = fmax_rs(hi[d], it.c[d] + it.r);
+        }
+    double cb[3] = {(lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5};
+    double rb = 0.0;
+    for (const Item& it : items) rb = fmax_rs(rb, dist(it.c, cb) + it.r);
+    if (rb < r) {
+        out_c[0] = cb[0]; out_c[1] = cb[1]; out_c[2] = cb[2]; *out_r = rb;
+    } else {
+        out_c[0] = c[0]; out_c[1] = c[1]; out_c[2] = c[2]; *out_r = r;
+    }
+}
+
+// build_rec, tree.rs:404-445
+static size_t build_rec(const std::vector<uint64_t>& keys, std::vector<Cell>& cells, uint32_t level,
+                        size_t start, size_t end, size_t n_leaf, uint32_t max_level) {
+    size_t count = end - start;
+    bool leaf = count <= n_leaf || level >= max_level;
+    Cell c;
+    c.first = start;
+    c.count = count;
+    for (int k = 0; k < 8; ++k) c.children[k] = -1;
+    c.leaf = leaf;
+    c.level = level;
+    c.cen[0] = c.cen[1] = c.cen[2] = 0.0;
+    c.mass = 0.0;
+    c.rho = 0.0;
+    cells.push_back(c);
+    size_t id = cells.size() - 1;
+    if (leaf) return id;
+    uint32_t shift = 3 * (max_level - (level + 1));
+    size_t lo = start;
+    for (uint64_t oct = 0; oct < 8; ++oct) {
+        size_t hi = lo;
+        while (hi < end && ((keys[hi] >> shift) & 7ULL) == oct) ++hi;
+        if (hi > lo) {
+            size_t cid = build_rec(keys, cells, level + 1, lo, hi, n_leaf, max_level);
+            cells[id].children[oct] = (int32_t)cid;
+        }
+        lo = hi;
+    }
+    return id;
+}
+
+// geometry, tree.rs:152-227 (+ com_of_slots :257-275, sphere_of_slots :278-286)
+static void geometry(Tree& t, const double* pos, const double* mass) {
+    for (size_t ii = t.cells.size(); ii-- > 0;) {
+        Cell cell = t.cells[ii];
+        bool is_leaf = true;
+        for (int k = 0; k < 8; ++k)
+            if (cell.children[k] >= 0) is_leaf = false;
+        double m = 0.0;
+        double cen[3];
+        double rho = 0.0;
+        if (is_leaf) {
+            for (size_t k = cell.first; k < cell.first + cell.count; ++k) m += mass[t.order[k]];
+            if (t.mode == CENTER_COM) {
+                double com[3] = {0.0, 0.0, 0.0};
+                for (size_t k = cell.first; k < cell.first + cell.count; ++k) {
+                    uint32_t id = t.order[k];
+                    for (int d = 0; d < 3; ++d) com[d] += mass[id] * pos[3 * id + d];
+                }
+                for (int d = 0; d < 3; ++d) cen[d] = com[d] / m;
+            } else {
+                std::vector<Item> items(cell.count);
+                for (size_t k = 0; k < cell.count; ++k) {
+                    uint32_t id = t.order[cell.first + k];
+                    for (int d = 0; d < 3; ++d) items[k].c[d] = pos[3 * id + d];
+                    items[k].r = 0.0;
+                }
+                double r;
+                ritter(items, cen, &r);
+            }
+            for (size_t k = cell.first; k < cell.first + cell.count; ++k) {
+                uint32_t id = t.order[k];
+                rho = fmax_rs(rho, dist(&pos[3 * id], cen));
+            }
+        } else {
+            for (int k = 0; k < 8; ++k)
+                if (cell.children[k] >= 0) m += t.cells[cell.children[k]].mass;
+            if (t.mode == CENTER_COM) {
+                double com[3] = {0.0, 0.0, 0.0};
+                for (int k = 0; k < 8; ++k) {
+                    int c = cell.children[k];
+                    if (c < 0) continue;
+                    const Cell& ch = t.cells[c];
+                    for (int d = 0; d < 3; ++d) com[d] += ch.mass * ch.cen[d];
+                }
+                for (int d = 0; d < 3; ++d) cen[d] = com[d] / m;
+            } else {
+                std::vector<Item> items;
+                for (int k = 0; k < 8; ++k) {
+                    int c = cell.children[k];
+                    if (c < 0) continue;
+                    Item it;
+                    for (int d = 0; d < 3; ++d) it.c[d] = t.cells[c].cen[d];
+                    it.r = t.cells[c].rho;
+                    items.push_back(it);
+                }
+                double r;
+                ritter(items, cen, &r);
+            }
+            for (int k = 0; k < 8; ++k) {
+                int c = cell.children[k];
+                if (c < 0) continue;
+                const Cell& ch = t.cells[c];
+                rho = fmax_rs(rho, ch.rho + dist(ch.cen, cen));
+            }
+        }
+        t.cells[ii].mass = m;
+        t.cells[ii].cen[0] = cen[0];
+        t.cells[ii].cen[1] = cen[1];
+        t.cells[ii].cen[2] = cen[2];
+        t.cells[ii].rho = rho;
+    }
+}
+
+// refresh_with_mode, tree.rs:94-148. The key sort is stable (the reference's
+// sort_unstable_by_key leaves equal keys in unspecified order).
+static void build_tree(Tree& t, size_t n, const double* pos, const double* mass, size_t n_leaf, int mode) {
+    t.n_leaf = n_leaf;
+    t.mode = mode;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin_rs(lo[d], pos[3 * i + d]);
+            hi[d] = fmax_rs(hi[d], pos[3 * i + d]);
+        }
+    double side = fmax_rs(fmax_rs(fmax_rs(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]),
+                          std::numeric_limits<double>::min());
+    double inv_side = 1.0 / side;
+    for (int d = 0; d < 3; ++d) { t.lo[d] = lo[d]; t.hi[d] = hi[d]; }
+    t.side = side;
+    t.inv_side = inv_side;
+    std::vector<uint64_t> keys(n);
+    for (size_t i = 0; i < n; ++i)
+        keys[i] = morton_key(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], lo[0], inv_side);
+    std::vector<uint32_t> ix(n);
+    for (size_t i = 0; i < n; ++i) ix[i] = (uint32_t)i;
+    std::stable_sort(ix.begin(), ix.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+    t.order = ix;
+    t.keys_sorted.resize(n);
+    for (size_t k = 0; k < n; ++k) t.keys_sorted[k] = keys[ix[k]];
+    t.cells.clear();
+    build_rec(t.keys_sorted, t.cells, 0, 0, n, n_leaf, BITS);
+    geometry(t, pos, mass);
+}
+
+// ---------------------------------------------------------------- bodies.rs
+struct Bodies {  // bodies.rs:13-73 (slot order)
+    std::vector<double> x, y, z, m, ax, ay, az, pot;
+    void from_parts(size_t n, const double* pos, const double* mass, const std::vector<uint32_t>& order) {
+        x.assign(n, 0.0); y.assign(n, 0.0); z.assign(n, 0.0); m.assign(n, 0.0);
+        ax.assign(n, 0.0); ay.assign(n, 0.0); az.assign(n, 0.0); pot.assign(n, 0.0);
+        for (size_t k = 0; k < n; ++k) {
+            uint32_t id = order[k];
+            x[k] = pos[3 * id]; y[k] = pos[3 * id + 1]; z[k] = pos[3 * id + 2]; m[k] = mass[id];
+        }
+    }
+};
+
+// ---------------------------------------------------------------- moments.rs
+static std::vector<double> factorials(size_t p) {  // moments.rs:11-17
+    std::vector<double> f(2 * p + 1, 1.0);
+    for (size_t i = 1; i < f.size(); ++i) f[i] = f[i - 1] * (double)i;
+    return f;
+}
+static std::vector<double> binomials(size_t p) {  // moments.rs:20-27
+    std::vector<double> fact = factorials(p);
+    std::vector<double> b(p + 1, 1.0);
+    for (size_t k = 0; k <= p; ++k) b[k] = fact[p] / (fact[k] * fact[p - k]);
+    return b;
+}
+
+// p2m_cell, moments.rs:30-53
+static void p2m_cell(const Bodies& b, const Tree& t, size_t c, size_t p, Cx* moments, Cx* u) {
+    size_t d = dimp(p);
+    const Cell& cell = t.cells[c];
+    size_t off = c * d;
+    for (size_t k = cell.first; k < cell.first + cell.count; ++k) {
+        double r[3] = {b.x[k] - cell.cen[0], b.y[k] - cell.cen[1], b.z[k] - cell.cen[2]};
+        upsilon_table(r, p, u);
+        double m = b.m[k];
+        for (size_t i = 0; i < d; ++i) moments[off + i] = cadd(moments[off + i], cscale(u[i], m));
+    }
+}
+
+// m2m_cell, moments.rs:56-90
+static void m2m_cell(const Tree& t, size_t c, size_t p, Cx* moments, Cx* u) {
+    size_t d = dimp(p);
+    const Cell& cell = t.cells[c];
+    size_t off = c * d;
+    for (int o = 0; o < 8; ++o) {
+        int ch = cell.children[o];
+        if (ch < 0) continue;
+        const Cell& child = t.cells[ch];
+        double dv[3] = {child.cen[0] - cell.cen[0], child.cen[1] - cell.cen[1], child.cen[2] - cell.cen[2]};
+        upsilon_table(dv, p, u);
+        size_t coff = (size_t)ch * d;
+        for (size_t n = 0; n <= p; ++n) {
+            for (long m = -(long)n; m <= (long)n; ++m) {
+                Cx s = CZERO;
+                for (size_t k = 0; k <= n; ++k) {
+                    size_t nk = n - k;
+                    long lo = std::max(-(long)k, m - (long)nk);
+                    long hi = std::min((long)k, m + (long)nk);
+                    for (long l = lo; l <= hi; ++l) s = cadd(s, cmul(u[idx(k, l)], moments[coff + idx(nk, m - l)]));
+                }
+                moments[off + idx(n, m)] = cadd(moments[off + idx(n, m)], s);
+            }
+        }
+    }
+}
+
+// compute_moments, moments.rs:96-108 (the level-parallel variant :114-146 is
+// bit-identical; cells of one level are independent)
+static void compute_moments(const Bodies& b, const Tree& t, size_t p, Cx* moments) {
+    std::vector<Cx> u(dimp(p));
+    for (size_t c = t.cells.size(); c-- > 0;) {
+        if (t.cells[c].leaf) p2m_cell(b, t, c, p, moments, u.data());
+        else m2m_cell(t, c, p, moments, u.data());
+    }
+}
+
+// multipole_power, moments.rs:150-168
+static std::vector<double> multipole_power(const Cx* moments, size_t ncells, size_t p) {
+    size_t d = dimp(p);
+    std::vector<double> fact = factorials(p);
+    std::vector<double> pp(ncells * (p + 1), 0.0);
+    for (size_t c = 0; c < ncells; ++c) {
+        size_t off = c * d;
+        for (size_t n = 0; n <= p; ++n) {
+            double s = 0.0;
+            for (long m = -(long)n; m <= (long)n; ++m) {
+                size_t am = (size_t)std::labs(m);
+                Cx mc = moments[off + idx(n, m)];
+                double w = fact[n - am] * fact[n + am];
+                s += w * (mc.re * mc.re + mc.im * mc.im);
+            }
+            pp[c * (p + 1) + n] = std::sqrt(s);
+        }
+    }
+    return pp;
+}
+
+// ---------------------------------------------------------------- mac.rs
+enum MacMode { MAC_DEHNEN = 0, MAC_THETA = 1 };
+
+struct MacCtx {
+    int mode;
+    double eps;    // Dehnen accuracy parameter (reference `eps`)
+    double theta;  // geometric opening angle (extension)
+    size_t p;
+    const std::vector<Cell>* cells;
+    const double* pows;
+    const double* binom;
+    const double* fmin;
+};
+
+// error_estimate + accept, mac.rs:23-95
+static bool accept_dehnen(const MacCtx& mc, size_t ai, size_t bi) {
+    const Cell& ca = (*mc.cells)[ai];
+    const Cell& cb = (*mc.cells)[bi];
+    double dx = cb.cen[0] - ca.cen[0];
+    double dy = cb.cen[1] - ca.cen[1];
+    double dz = cb.cen[2] - ca.cen[2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double sum_rho = ca.rho + cb.rho;
+    if (r2 <= sum_rho * sum_rho) return false;
+    double r = std::sqrt(r2);
+    if (r == 0.0) return false;
+    size_t p = mc.p;
+    double rr2 = r * r;
+    double rp = 1.0;
+    for (size_t i = 0; i < p / 2; ++i) rp *= rr2;
+    if (p % 2 == 1) rp *= r;
+    double rpows[64];
+    rpows[0] = 1.0;
+    for (size_t j = 1; j <= p; ++j) rpows[j] = rpows[j - 1] * cb.rho;
+    size_t base = ai * (p + 1);
+    double s = 0.0;
+    for (size_t k = 0; k <= p; ++k) s += mc.binom[k] * mc.pows[base + k] * rpows[p - k];
+    double e = s / (ca.mass * rp);
+    double denom = ca.rho + cb.rho;
+    double est;
+    if (denom == 0.0) est = 0.0;
+    else est = 8.0 * fmax_rs(ca.rho, cb.rho) / denom * e;
+    if (est == 0.0) return true;
+    return est * ca.mass / r2 < mc.eps * mc.fmin[bi];
+}
+
+// Geometric MAC (extension): accept when (rho_A + rho_B) / r < theta.
+static bool accept_theta(const MacCtx& mc, size_t ai, size_t bi) {
+    const Cell& ca = (*mc.cells)[ai];
+    const Cell& cb = (*mc.cells)[bi];
+    double dx = cb.cen[0] - ca.cen[0];
+    double dy = cb.cen[1] - ca.cen[1];
+    double dz = cb.cen[2] - ca.cen[2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double sum_rho = ca.rho + cb.rho;
+    double r = std::sqrt(r2);
+    return sum_rho < mc.theta * r;
+}
+
+static inline bool accept(const MacCtx& mc, size_t a, size_t b) {
+    return mc.mode == MAC_DEHNEN ? accept_dehnen(mc, a, b) : accept_theta(mc, a, b);
+}
+
+// f_walk, mac.rs:99-147
+static double f_walk(const Bodies& b, const Tree& t, size_t i, std::vector<size_t>& stack) {
+    double pb[3] = {b.x[i], b.y[i], b.z[i]};
+    stack.clear();
+    stack.push_back(0);
+    double fi = 0.0;
+    while (!stack.empty()) {
+        size_t c = stack.back();
+        stack.pop_back();
+        const Cell& cell = t.cells[c];
+        if (cell.leaf) {
+            size_t below = std::min(i, cell.first + cell.count);
+            size_t above = std::max(cell.first, i + 1);
+            for (size_t k = cell.first; k < below; ++k) {
+                double dx = pb[0] - b.x[k], dy = pb[1] - b.y[k], dz = pb[2] - b.z[k];
+                double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > 0.0) fi += b.m[k] / r2;
+            }
+            for (size_t k = above; k < cell.first + cell.count; ++k) {
+                double dx = pb[0] - b.x[k], dy = pb[1] - b.y[k], dz = pb[2] - b.z[k];
+                double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > 0.0) fi += b.m[k] / r2;
+            }
+        } else {
+            double dx = pb[0] - cell.cen[0], dy = pb[1] - cell.cen[1], dz = pb[2] - cell.cen[2];
+            double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 > cell.rho * cell.rho) {
+                fi += cell.mass / d2;
+            } else {
+                for (int k = 0; k < 8; ++k)
+                    if (cell.children[k] >= 0) stack.push_back((size_t)cell.children[k]);
+            }
+        }
+    }
+    return fi;
+}
+
+// fmin_of, mac.rs:151-173
+static std::vector<double> fmin_of(const std::vector<double>& f, const Tree& t) {
+    size_t nc = t.cells.size();
+    std::vector<double> fm(nc, INFINITY);
+    for (size_t c = nc; c-- > 0;) {
+        const Cell& cell = t.cells[c];
+        double m = INFINITY;
+        if (cell.leaf) {
+            for (size_t k = cell.first; k < cell.first + cell.count; ++k) m = fmin_rs(m, f[k]);
+        } else {
+            for (int k = 0; k < 8; ++k)
+                if (cell.children[k] >= 0) m = fmin_rs(m, fm[cell.children[k]]);
+        }
+        fm[c] = m;
+    }
+    return fm;
+}
+
+// f_prepass (mac.rs:177-186) and f_prepass_par (:192-213, bit-identical)
+static void f_prepass(const Bodies& b, const Tree& t, std::vector<double>& f, std::vector<double>& fmin,
+                      int nthreads) {
+    size_t n = b.x.size();
+    f.assign(n, 0.0);
+    if (nthreads <= 1) {
+        std::vector<size_t> stack;
+        stack.reserve(64);
+        for (size_t i = 0; i < n; ++i) f[i] = f_walk(b, t, i, stack);
+    } else {
+        std::vector<std::thread> th;
+        size_t chunk = (n + nthreads - 1) / nthreads;
+        for (int w = 0; w < nthreads; ++w) {
+            th.emplace_back([&, w]() {
+                std::vector<size_t> stack;
+                stack.reserve(64);
+                size_t lo = w * chunk, hi = std::min(n, lo + chunk);
+                for (size_t i = lo; i < hi; ++i) f[i] = f_walk(b, t, i, stack);
+            });
+        }
+        for (auto& x : th) x.join();
+    }
+    fmin = fmin_of(f, t);
+}
+
+// ---------------------------------------------------------------- translate.rs
+// m2l_mutual_scratch, translate.rs:47-136
+struct M2lScratch {
+    std::vector<Cx> th, ths, cma, cmb;
+    explicit M2lScratch(size_t p) : th(dimp(p)), ths(dimp(p)), cma(dimp(p)), cmb(dimp(p)) {}
+};
+
+static void m2l_mutual(const Tree& t, size_t a, size_t b, const Cx* moments, Cx* locals, size_t p,
+                       M2lScratch& sc) {
+    size_t d = dimp(p);
+    const Cell& ca = t.cells[a];
+    const Cell& cb = t.cells[b];
+    double r[3] = {cb.cen[0] - ca.cen[0], cb.cen[1] - ca.cen[1], cb.cen[2] - ca.cen[2]};
+    theta_table(r, p, sc.th.data());
+    size_t offa = a * d, offb = b * d;
+    for (size_t i = 0; i < d; ++i) {
+        sc.cma[i] = cconj(moments[offa + i]);
+        sc.cmb[i] = cconj(moments[offb + i]);
+    }
+    {
+        size_t o = 0;
+        for (size_t n = 0; n <= p; ++n) {
+            double sgn = (n % 2 == 0) ? 1.0 : -1.0;
+            for (size_t q = 0; q < 2 * n + 1; ++q) {
+                sc.ths[o] = cscale(sc.th[o], sgn);
+                ++o;
+            }
+        }
+    }
+    const Cx* th = sc.th.data();
+    const Cx* ths = sc.ths.data();
+    const Cx* cma = sc.cma.data();
+    const Cx* cmb = sc.cmb.data();
+    for (size_t n = 0; n <= p; ++n) {
+        long n2n = (long)(n * (n + 1));
+        for (long m = -(long)n; m <= (long)n; ++m) {
+            size_t nidx = (size_t)(n2n + m);
+            double fa_r = 0.0, fa_i = 0.0, fb_r = 0.0, fb_i = 0.0;
+            for (size_t k = 0; k <= p - n; ++k) {
+                size_t s = n + k;
+                long sk = (long)(s * (s + 1));
+                long kb = (long)(k * (k + 1));
+                long ki = (long)k;
+                size_t thx = (size_t)(sk + m - ki);
+                size_t i = (size_t)(kb - ki);
+                for (long l = -ki; l <= ki; ++l) {
+                    Cx tt = th[thx];
+                    Cx ts = ths[thx];
+                    Cx ma = cma[i];
+                    Cx mb = cmb[i];
+                    fb_r += ma.re * tt.re - ma.im * tt.im;
+                    fb_i += ma.re * tt.im + ma.im * tt.re;
+                    fa_r += mb.re * ts.re - mb.im * ts.im;
+                    fa_i += mb.re * ts.im + mb.im * ts.re;
+                    ++thx;
+                    ++i;
+                }
+            }
+            locals[offb + nidx] = cadd(locals[offb + nidx], cx(fb_r, fb_i));
+            locals[offa + nidx] = cadd(locals[offa + nidx], cx(fa_r, fa_i));
+        }
+    }
+}
+
+// l2l_into, translate.rs:175-206
+static void l2l(const Tree& t, size_t parent, size_t child, Cx* locals, size_t p, Cx* u) {
+    const Cell& cp = t.cells[parent];
+    const Cell& cc = t.cells[child];
+    double r[3] = {cp.cen[0] - cc.cen[0], cp.cen[1] - cc.cen[1], cp.cen[2] - cc.cen[2]};
+    upsilon_table(r, p, u);
+    size_t d = dimp(p);
+    size_t offp = parent * d, offc = child * d;
+    for (size_t n = 0; n <= p; ++n) {
+        for (long m = -(long)n; m <= (long)n; ++m) {
+            size_t nidx = idx(n, m);
+            Cx s = CZERO;
+            for (size_t k = 0; k <= p - n; ++k)
+                for (long l = -(long)k; l <= (long)k; ++l)
+                    s = cadd(s, cmul(cconj(u[idx(k, l)]), locals[offp + idx(n + k, m + l)]));
+            locals[offc + nidx] = cadd(locals[offc + nidx], s);
+        }
+    }
+}
+
+// l2l_down, translate.rs:209-218
+static void l2l_down(const Tree& t, Cx* locals, size_t p) {
+    std::vector<Cx> u(dimp(p));
+    for (size_t c = 0; c < t.cells.size(); ++c)
+        for (int k = 0; k < 8; ++k)
+            if (t.cells[c].children[k] >= 0) l2l(t, c, (size_t)t.cells[c].children[k], locals, p, u.data());
+}
+
+// l2p_into, translate.rs:271-309
+static void l2p(const Tree& t, size_t cell, const double pos[3], const Cx* locals, size_t p, double* pot,
+                double acc[3], Cx* u) {
+    const Cell& c = t.cells[cell];
+    double r[3] = {c.cen[0] - pos[0], c.cen[1] - pos[1], c.cen[2] - pos[2]};
+    upsilon_table(r, p, u);
+    size_t off = cell * dimp(p);
+    Cx psi00 = CZERO;
+    for (size_t k = 0; k <= p; ++k)
+        for (long l = -(long)k; l <= (long)k; ++l) psi00 = cadd(psi00, cmul(cconj(u[idx(k, l)]), locals[off + idx(k, l)]));
+    Cx psi11 = CZERO, psi10 = CZERO;
+    if (p >= 1) {
+        for (size_t k = 0; k <= p - 1; ++k)
+            for (long l = -(long)k; l <= (long)k; ++l) {
+                Cx uc = cconj(u[idx(k, l)]);
+                psi11 = cadd(psi11, cmul(uc, locals[off + idx(1 + k, 1 + l)]));
+                psi10 = cadd(psi10, cmul(uc, locals[off + idx(1 + k, l)]));
+            }
+    }
+    *pot += psi00.re;
+    acc[0] -= psi11.re;
+    acc[1] -= psi11.im;
+    acc[2] -= psi10.re;
+}
+
+// ---------------------------------------------------------------- rotation.rs
+static const size_t ROT_P = 20;  // rotation.rs:45
+static inline size_t blocksum(size_t p) { return (p + 1) * (4 * p * p + 8 * p + 3) / 3; }  // :49
+static inline size_t block_off(size_t j) { return j == 0 ? 0 : j * (4 * j * j - 1) / 3; }  // :55
+
+// dot_row with its 4-way accumulator split, rotation.rs:70-103
+static inline void dot_row(const double* w, const Cx* v, size_t nb, double* outr, double* outi) {
+    double a0r = 0, a0i = 0, a1r = 0, a1i = 0, a2r = 0, a2i = 0, a3r = 0, a3i = 0;
+    size_t c = 0;
+    while (c + 4 <= nb) {
+        a0r += w[c] * v[c].re; a0i += w[c] * v[c].im;
+        a1r += w[c + 1] * v[c + 1].re; a1i += w[c + 1] * v[c + 1].im;
+        a2r += w[c + 2] * v[c + 2].re; a2i += w[c + 2] * v[c + 2].im;
+        a3r += w[c + 3] * v[c + 3].re; a3i += w[c + 3] * v[c + 3].im;
+        c += 4;
+    }
+    double sr = (a0r + a1r) + (a2r + a3r);
+    double si = (a0i + a1i) + (a2i + a3i);
+    while (c < nb) {
+        sr += w[c] * v[c].re;
+        si += w[c] * v[c].im;
+        ++c;
+    }
+    *outr = sr;
+    *outi = si;
+}
+
+// RotCtx, rotation.rs:106-435
+struct RotCtx {
+    size_t p;
+    std::vector<double> fact, sw, swt;
+    std::vector<Cx> in_, out_, fin, fout, b, f, tmp, tmp2, pha, phb;
+    std::vector<double> facr;
+
+    explicit RotCtx(size_t p_) : p(p_) {
+        size_t d = dimp(p);
+        fact.assign(p + 1, 1.0);
+        for (size_t i = 1; i <= p; ++i) fact[i] = fact[i - 1] * (double)i;
+        std::vector<double> f2(2 * p + 1, 1.0);
+        for (size_t i = 1; i < f2.size(); ++i) f2[i] = f2[i - 1] * (double)i;
+        size_t bs = blocksum(p);
+        sw.assign(bs, 0.0);
+        swt.assign(bs, 0.0);
+        sw[0] = 1.0;
+        swt[0] = 1.0;
+        // Swap matrices B_n (Dehnen 2014 eq 63), rotation.rs:143-211
+        for (size_t n = 1; n <= p; ++n) {
+            size_t nb = 2 * n + 1, off = block_off(n), nbp = 2 * n - 1, offp = block_off(n - 1);
+            long nn = (long)n;
+            auto prev = [&](size_t row_base, long l) -> double {
+                // entry of B_{n-1} row `row_base` at column l (|l| <= n-1), else 0
+                if (std::labs(l) <= nn - 1) return sw[row_base + (size_t)(l + (nn - 1))];
+                return 0.0;
+            };
+            for (size_t mr = 0; mr < nb; ++mr) {
+                long m = (long)mr - nn;
+                size_t row = off + mr * nb;
+                size_t row_prev = offp + (mr == 0 ? 0 : mr - 1) * nbp;
+                for (size_t lc = 0; lc < nb; ++lc) {
+                    long l = (long)lc - nn;
+                    double v;
+                    if (std::labs(m) <= nn - 1) {
+                        double a = prev(row_prev, l - 1);
+                        double bb = prev(row_prev, l + 1);
+                        v = (a - bb) * 0.5;
+                    } else if (m == nn) {
+                        size_t src = offp + (2 * n - 2) * nbp;
+                        double a = prev(src, l - 1), bb = prev(src, l + 1), c = prev(src, l);
+                        v = (a + bb + 2.0 * c) * 0.5;
+                    } else {
+                        size_t src = offp;
+                        double a = prev(src, l - 1), bb = prev(src, l + 1), c = prev(src, l);
+                        v = (a + bb - 2.0 * c) * 0.5;
+                    }
+                    sw[row + lc] = v;
+                    swt[off + lc * nb + mr] = v;
+                }
+            }
+        }
+        in_.assign(d, CZERO); out_.assign(d, CZERO); fin.assign(d, CZERO); fout.assign(d, CZERO);
+        for (size_t n = 0; n <= p; ++n) {
+            for (long m = -(long)n; m <= (long)n; ++m) {
+                size_t i = idx(n, m);
+                size_t am = (size_t)std::labs(m);
+                double fm = f2[n - am] * f2[n + am];
+                Cx ei;
+                switch (((m % 4) + 4) % 4) {
+                    case 0: ei = cx(1.0, 0.0); break;
+                    case 1: ei = cx(0.0, -1.0); break;
+                    case 2: ei = cx(-1.0, 0.0); break;
+                    default: ei = cx(0.0, 1.0); break;
+                }
+                in_[i] = cscale(ei, fm);
+                out_[i] = cscale(cconj(ei), 1.0 / fm);
+                fin[i] = cscale(ei, 1.0 / fm);
+                fout[i] = cscale(cconj(ei), fm);
+            }
+        }
+        b.assign(d, CZERO); f.assign(d, CZERO);
+        tmp.assign(2 * p + 1, CZERO); tmp2.assign(2 * p + 1, CZERO);
+        pha.assign(2 * p + 1, CZERO); phb.assign(2 * p + 1, CZERO);
+        facr.assign(p + 1, 0.0);
+    }
+
+    // m2l_pair, rotation.rs:262-301
+    void m2l_pair(const Tree& t, size_t a, size_t bcell, const Cx* moments, Cx* locals) {
+        size_t d = dimp(p);
+        const Cell& ca = t.cells[a];
+        const Cell& cb = t.cells[bcell];
+        double r[3] = {cb.cen[0] - ca.cen[0], cb.cen[1] - ca.cen[1], cb.cen[2] - ca.cen[2]};
+        double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        double rinv = 1.0 / std::sqrt(r2);
+        double alpha = std::atan2(r[1], r[0]);
+        double s_beta = std::sqrt(r[0] * r[0] + r[1] * r[1]);
+        double beta = std::atan2(s_beta, r[2]);
+        double irp = rinv;
+        for (size_t j = 0; j <= p; ++j) {
+            facr[j] = fact[j] * irp;
+            irp *= rinv;
+        }
+        for (long m = -(long)p; m <= (long)p; ++m) {
+            double aa = (double)m * alpha;
+            pha[(size_t)(m + (long)p)] = cx(std::cos(aa), std::sin(aa));
+            double bb = (double)m * beta;
+            phb[(size_t)(m + (long)p)] = cx(std::cos(bb), std::sin(bb));
+        }
+        apply(a * d, bcell * d, moments, locals);
+        for (size_t i = 0; i < pha.size(); ++i) {
+            long m = (long)i - (long)p;
+            double sgn = (((m % 2) + 2) % 2 == 0) ? 1.0 : -1.0;
+            pha[i] = cscale(pha[i], sgn);
+            phb[i] = cscale(cconj(phb[i]), sgn);
+        }
+        apply(bcell * d, a * d, moments, locals);
+    }
+
+    // apply, rotation.rs:319-435
+    void apply(size_t so, size_t do_, const Cx* moments, Cx* locals) {
+        for (size_t k = 0; k <= p; ++k) {
+            size_t nb = 2 * k + 1, k2 = k * k, off = block_off(k), po = p - k;
+            for (size_t c = 0; c < nb; ++c) {
+                Cx m = moments[so + k2 + c];
+                Cx ph = pha[po + c];
+                Cx iv = in_[k2 + c];
+                double vr = m.re * ph.re + m.im * ph.im;
+                double vi = m.re * ph.im - m.im * ph.re;
+                tmp[c] = cx(vr * iv.re - vi * iv.im, vr * iv.im + vi * iv.re);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                double sr, si;
+                dot_row(&sw[off + r * nb], tmp.data(), nb, &sr, &si);
+                tmp2[r] = cx(sr, si);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                Cx pbb = phb[po + r];
+                Cx s = tmp2[r];
+                tmp2[r] = cx(s.re * pbb.re - s.im * pbb.im, s.re * pbb.im + s.im * pbb.re);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                double sr, si;
+                dot_row(&sw[off + r * nb], tmp2.data(), nb, &sr, &si);
+                Cx ov = out_[k2 + r];
+                b[k2 + r] = cx(sr * ov.re - si * ov.im, sr * ov.im + si * ov.re);
+            }
+        }
+        for (size_t n = 0; n <= p; ++n) {
+            size_t nb = 2 * n + 1, n2 = n * n;
+            for (size_t r = 0; r < nb; ++r) {
+                long m = (long)r - (long)n;
+                size_t am = (size_t)std::labs(m);
+                double fr = 0.0, fi = 0.0;
+                for (size_t k = am; k <= p - n; ++k) {
+                    Cx bv = b[k * k + (size_t)((long)k - m)];
+                    double fv = facr[n + k];
+                    fr += bv.re * fv;
+                    fi += bv.im * fv;
+                }
+                f[n2 + r] = cx(fr, fi);
+            }
+        }
+        for (size_t n = 0; n <= p; ++n) {
+            size_t nb = 2 * n + 1, off = block_off(n), n2 = n * n, po = p - n;
+            for (size_t c = 0; c < nb; ++c) {
+                Cx fv = f[n2 + c];
+                Cx iv = fin[n2 + c];
+                tmp[c] = cx(fv.re * iv.re - fv.im * iv.im, fv.re * iv.im + fv.im * iv.re);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                double sr, si;
+                dot_row(&swt[off + r * nb], tmp.data(), nb, &sr, &si);
+                tmp2[r] = cx(sr, si);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                Cx pb = phb[po + r];
+                Cx s = tmp2[r];
+                tmp2[r] = cx(s.re * pb.re + s.im * pb.im, s.im * pb.re - s.re * pb.im);
+            }
+            for (size_t r = 0; r < nb; ++r) {
+                double sr, si;
+                dot_row(&swt[off + r * nb], tmp2.data(), nb, &sr, &si);
+                Cx ov = fout[n2 + r];
+                Cx pv = pha[po + r];
+                Cx acc = cx(sr * ov.re - si * ov.im, sr * ov.im + si * ov.re);
+                Cx cur = locals[do_ + n2 + r];
+                Cx add = cx(acc.re * pv.re - acc.im * pv.im, acc.re * pv.im + acc.im * pv.re);
+                locals[do_ + n2 + r] = cx(cur.re + add.re, cur.im + add.im);
+            }
+        }
+    }
+};
+
+// ---------------------------------------------------------------- p2p.rs
+// p2p_self_scalar, p2p.rs:13-46 (+ Plummer softening extension: r2 += soft2)
+static void p2p_self(Bodies& b, size_t first, size_t count, double soft2) {
+    for (size_t i = 0; i < count; ++i) {
+        double xi = b.x[first + i], yi = b.y[first + i], zi = b.z[first + i], mi = b.m[first + i];
+        double axi = 0.0, ayi = 0.0, azi = 0.0, poti = 0.0;
+        for (size_t j = i + 1; j < count; ++j) {
+            double dx = b.x[first + j] - xi, dy = b.y[first + j] - yi, dz = b.z[first + j] - zi;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (soft2 != 0.0) r2 = r2 + soft2;
+            double inv = 1.0 / std::sqrt(r2);
+            double inv3 = inv * inv * inv;
+            double mj = b.m[first + j];
+            axi += mj * inv3 * dx;
+            ayi += mj * inv3 * dy;
+            azi += mj * inv3 * dz;
+            poti += mj * inv;
+            double fm = mi * inv3;
+            b.ax[first + j] -= fm * dx;
+            b.ay[first + j] -= fm * dy;
+            b.az[first + j] -= fm * dz;
+            b.pot[first + j] += mi * inv;
+        }
+        b.ax[first + i] += axi;
+        b.ay[first + i] += ayi;
+        b.az[first + i] += azi;
+        b.pot[first + i] += poti;
+    }
+}
+
+// p2p_pair_scalar, p2p.rs:49-88
+static void p2p_pair(Bodies& b, size_t af, size_t ac, size_t bf, size_t bc, double soft2) {
+    for (size_t i = 0; i < ac; ++i) {
+        double xi = b.x[af + i], yi = b.y[af + i], zi = b.z[af + i], mi = b.m[af + i];
+        double axi = 0.0, ayi = 0.0, azi = 0.0, poti = 0.0;
+        for (size_t j = 0; j < bc; ++j) {
+            double dx = b.x[bf + j] - xi, dy = b.y[bf + j] - yi, dz = b.z[bf + j] - zi;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (soft2 != 0.0) r2 = r2 + soft2;
+            double inv = 1.0 / std::sqrt(r2);
+            double inv3 = inv * inv * inv;
+            double mj = b.m[bf + j];
+            axi += mj * inv3 * dx;
+            ayi += mj * inv3 * dy;
+            azi += mj * inv3 * dz;
+            poti += mj * inv;
+            double fm = mi * inv3;
+            b.ax[bf + j] -= fm * dx;
+            b.ay[bf + j] -= fm * dy;
+            b.az[bf + j] -= fm * dz;
+            b.pot[bf + j] += mi * inv;
+        }
+        b.ax[af + i] += axi;
+        b.ay[af + i] += ayi;
+        b.az[af + i] += azi;
+        b.pot[af + i] += poti;
+    }
+}
+
+// ---------------------------------------------------------------- walk.rs
+struct WalkOut {
+    std::vector<uint32_t> m2l;  // flat (a, b) pairs in emission order
+    std::vector<uint32_t> p2p;  // flat (a, b) pairs incl. self (a, a)
+    uint64_t pops = 0;
+};
+
+// process_pair / process_stack / dual_walk, walk.rs:94-255. With `evaluate`
+// false only the lists are recorded (the record phase of walk.rs:342-488).
+static void dual_walk(Bodies& b, const Tree& t, const MacCtx& mc, const Cx* moments, Cx* locals, RotCtx* rot,
+                      bool evaluate, double soft2, WalkOut& out) {
+    size_t p = mc.p;
+    M2lScratch sc(p);
+    std::vector<std::pair<size_t, size_t>> stack;
+    stack.reserve(1024);
+    stack.push_back({0, 0});
+    while (!stack.empty()) {
+        auto pr = stack.back();
+        stack.pop_back();
+        size_t a = pr.first, bb = pr.second;
+        out.pops++;
+        const Cell& ca = t.cells[a];
+        const Cell& cb = t.cells[bb];
+        if (a == bb) {
+            if (ca.leaf) {
+                out.p2p.push_back((uint32_t)a);
+                out.p2p.push_back((uint32_t)a);
+                if (evaluate) p2p_self(b, ca.first, ca.count, soft2);
+            } else {
+                for (int i = 0; i < 8; ++i) {
+                    if (ca.children[i] < 0) continue;
+                    for (int j = i; j < 8; ++j)
+                        if (ca.children[j] >= 0) stack.push_back({(size_t)ca.children[i], (size_t)ca.children[j]});
+                }
+            }
+        } else if (accept(mc, a, bb) && accept(mc, bb, a)) {
+            out.m2l.push_back((uint32_t)a);
+            out.m2l.push_back((uint32_t)bb);
+            if (evaluate) {
+                if (p >= ROT_P && rot) rot->m2l_pair(t, a, bb, moments, locals);
+                else m2l_mutual(t, a, bb, moments, locals, p, sc);
+            }
+        } else if (ca.leaf && cb.leaf) {
+            out.p2p.push_back((uint32_t)a);
+            out.p2p.push_back((uint32_t)bb);
+            if (evaluate) p2p_pair(b, ca.first, ca.count, cb.first, cb.count, soft2);
+        } else if (ca.leaf) {
+            for (int j = 0; j < 8; ++j)
+                if (cb.children[j] >= 0) stack.push_back({a, (size_t)cb.children[j]});
+        } else if (cb.leaf) {
+            for (int i = 0; i < 8; ++i)
+                if (ca.children[i] >= 0) stack.push_back({(size_t)ca.children[i], bb});
+        } else {
+            if (ca.rho >= cb.rho) {
+                for (int i = 0; i < 8; ++i)
+                    if (ca.children[i] >= 0) stack.push_back({(size_t)ca.children[i], bb});
+            } else {
+                for (int j = 0; j < 8; ++j)
+                    if (cb.children[j] >= 0) stack.push_back({a, (size_t)cb.children[j]});
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- direct.rs
+// direct, direct.rs:6-31 (+ softening extension)
+static void direct(size_t n, const double* pos, const double* mass, double soft2, double* acc, double* pot) {
+    for (size_t i = 0; i < 3 * n; ++i) acc[i] = 0.0;
+    for (size_t i = 0; i < n; ++i) pot[i] = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t j = i + 1; j < n; ++j) {
+            const double* pa = &pos[3 * i];
+            const double* pb = &pos[3 * j];
+            double dx = pb[0] - pa[0], dy = pb[1] - pa[1], dz = pb[2] - pa[2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (soft2 != 0.0) r2 = r2 + soft2;
+            double inv = 1.0 / std::sqrt(r2);
+            double inv3 = inv * inv * inv;
+            acc[3 * i + 0] += mass[j] * inv3 * dx;
+            acc[3 * i + 1] += mass[j] * inv3 * dy;
+            acc[3 * i + 2] += mass[j] * inv3 * dz;
+            acc[3 * j + 0] -= mass[i] * inv3 * dx;
+            acc[3 * j + 1] -= mass[i] * inv3 * dy;
+            acc[3 * j + 2] -= mass[i] * inv3 * dz;
+            pot[i] += mass[j] * inv;
+            pot[j] += mass[i] * inv;
+        }
+    }
+}
+
+// One-sided direct sum for selected targets (the sampled-error loop of
+// crates/bench/src/main.rs:34-78, generalised to a target list and softening).
+static void direct_targets(size_t n, const double* pos, const double* mass, double soft2, size_t nt,
+                           const uint32_t* tgt, double* acc, double* pot, double* fsc, int nthreads) {
+    auto work = [&](size_t lo, size_t hi) {
+        for (size_t q = lo; q < hi; ++q) {
+            size_t i = tgt[q];
+            double ax = 0, ay = 0, az = 0, f = 0, ph = 0;
+            const double* pi = &pos[3 * i];
+            for (size_t j = 0; j < n; ++j) {
+                if (j == i) continue;
+                const double* pj = &pos[3 * j];
+                double dx = pj[0] - pi[0], dy = pj[1] - pi[1], dz = pj[2] - pi[2];
+                double r2 = dx * dx + dy * dy + dz * dz;
+                if (soft2 != 0.0) r2 = r2 + soft2;
+                double inv = 1.0 / std::sqrt(r2);
+                double inv2 = inv * inv;
+                double inv3 = inv2 * inv;
+                ax += mass[j] * inv3 * dx;
+                ay += mass[j] * inv3 * dy;
+                az += mass[j] * inv3 * dz;
+                f += mass[j] * inv2;
+                ph += mass[j] * inv;
+            }
+            acc[3 * q] = ax; acc[3 * q + 1] = ay; acc[3 * q + 2] = az;
+            if (pot) pot[q] = ph;
+            if (fsc) fsc[q] = f;
+        }
+    };
+    if (nthreads <= 1) { work(0, nt); return; }
+    std::vector<std::thread> th;
+    size_t chunk = (nt + nthreads - 1) / nthreads;
+    for (int w = 0; w < nthreads; ++w) {
+        size_t lo = w * chunk, hi = std::min(nt, lo + chunk);
+        if (lo < hi) th.emplace_back(work, lo, hi);
+    }
+    for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------- fmm.rs
+struct Fmm {
+    Tree tree;
+    size_t p;
+    MacCtx mc;
+    double mac_eps, theta, soft2;
+    int mac_mode;
+    // retained intermediates of the last run (for parity checks)
+    size_t n = 0;
+    std::vector<Cx> moments, locals_walk, locals;
+    std::vector<double> pows, binom, f, fmin;
+    Bodies bodies_near;
+    WalkOut lists;
+};
+
+// run_impl, fmm.rs:69-142. nthreads == 1 is the reference's serial run; more
+// threads parallelise the independent phases (bit-identical moments, f pre-pass,
+// L2L and L2P; walk replay in parallel with per-thread accumulators reduced in
+// thread order, as walk.rs:490-622 does).
+static void run(Fmm& F, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot) {
+    const Tree& t = F.tree;
+    size_t p = F.p, d = dimp(p), nc = t.cells.size();
+    F.n = n;
+    Bodies& b = F.bodies_near;
+    b.from_parts(n, pos, mass, t.order);
+    F.moments.assign(nc * d, CZERO);
+    if (nthreads <= 1) {
+        compute_moments(b, t, p, F.moments.data());
+    } else {
+        // level-parallel, deepest level first (moments.rs:114-146)
+        uint32_t maxl = 0;
+        for (const Cell& c : t.cells) maxl = std::max(maxl, c.level);
+        std::vector<std::vector<size_t>> lv(maxl + 1);
+        for (size_t c = 0; c < nc; ++c) lv[t.cells[c].level].push_back(c);
+        for (size_t L = maxl + 1; L-- > 0;) {
+            auto& cs = lv[L];
+            std::atomic<size_t> next(0);
+            std::vector<std::thread> th;
+            for (int w = 0; w < nthreads; ++w)
+                th.emplace_back([&]() {
+                    std::vector<Cx> u(d);
+                    size_t q;
+                    while ((q = next.fetch_add(64)) < cs.size()) {
+                        for (size_t e = q; e < std::min(cs.size(), q + 64); ++e) {
+                            size_t c = cs[e];
+                            if (t.cells[c].leaf) p2m_cell(b, t, c, p, F.moments.data(), u.data());
+                            else m2m_cell(t, c, p, F.moments.data(), u.data());
+                        }
+                    }
+                });
+            for (auto& x : th) x.join();
+        }
+    }
+    F.pows = multipole_power(F.moments.data(), nc, p);
+    F.binom = binomials(p);
+    if (F.mac_mode == MAC_DEHNEN) {
+        f_prepass(b, t, F.f, F.fmin, nthreads);
+    } else {
+        F.f.assign(n, 0.0);
+        F.fmin.assign(nc, INFINITY);
+    }
+    F.mc.mode = F.mac_mode;
+    F.mc.eps = F.mac_eps;
+    F.mc.theta = F.theta;
+    F.mc.p = p;
+    F.mc.cells = &t.cells;
+    F.mc.pows = F.pows.data();
+    F.mc.binom = F.binom.data();
+    F.mc.fmin = F.fmin.data();
+    std::vector<Cx> locals(nc * d, CZERO);
+    F.lists = WalkOut();
+    if (nthreads <= 1) {
+        RotCtx* rot = nullptr;
+        RotCtx rc(p >= ROT_P ? p : 0);
+        if (p >= ROT_P) rot = &rc;
+        dual_walk(b, t, F.mc, F.moments.data(), locals.data(), rot, true, F.soft2, F.lists);
+    } else {
+        dual_walk(b, t, F.mc, F.moments.data(), locals.data(), nullptr, false, F.soft2, F.lists);
+        const std::vector<uint32_t>& m2l = F.lists.m2l;
+        const std::vector<uint32_t>& pp = F.lists.p2p;
+        size_t nm = m2l.size() / 2, np = pp.size() / 2;
+        std::vector<std::vector<Cx>> tl(nthreads);
+        std::vector<Bodies> tb(nthreads);
+        std::vector<std::thread> th;
+        for (int w = 0; w < nthreads; ++w)
+            th.emplace_back([&, w]() {
+                tl[w].assign(nc * d, CZERO);
+                tb[w] = b;
+                M2lScratch sc(p);
+                RotCtx rc(p >= ROT_P ? p : 0);
+                size_t lo = nm * w / nthreads, hi = nm * (w + 1) / nthreads;
+                for (size_t q = lo; q < hi; ++q) {
+                    size_t a = m2l[2 * q], bb = m2l[2 * q + 1];
+                    if (p >= ROT_P) rc.m2l_pair(t, a, bb, F.moments.data(), tl[w].data());
+                    else m2l_mutual(t, a, bb, F.moments.data(), tl[w].data(), p, sc);
+                }
+                size_t plo = np * w / nthreads, phi = np * (w + 1) / nthreads;
+                for (size_t q = plo; q < phi; ++q) {
+                    size_t a = pp[2 * q], bb = pp[2 * q + 1];
+                    const Cell& ca = t.cells[a];
+                    const Cell& cb = t.cells[bb];
+                    if (a == bb) p2p_self(tb[w], ca.first, ca.count, F.soft2);
+                    else p2p_pair(tb[w], ca.first, ca.count, cb.first, cb.count, F.soft2);
+                }
+            });
+        for (auto& x : th) x.join();
+        th.clear();
+        size_t total = nc * d;
+        for (int w = 0; w < nthreads; ++w)
+            th.emplace_back([&, w]() {
+                size_t lo = total * w / nthreads, hi = total * (w + 1) / nthreads;
+                for (size_t i = lo; i < hi; ++i) {
+                    Cx a = locals[i];
+                    for (int v = 0; v < nthreads; ++v) a = cadd(a, tl[v][i]);
+                    locals[i] = a;
+                }
+                size_t blo = n * w / nthreads, bhi = n * (w + 1) / nthreads;
+                for (size_t k = blo; k < bhi; ++k) {
+                    double sx = 0, sy = 0, sz = 0, sp = 0;
+                    for (int v = 0; v < nthreads; ++v) {
+                        sx += tb[v].ax[k]; sy += tb[v].ay[k]; sz += tb[v].az[k]; sp += tb[v].pot[k];
+                    }
+                    b.ax[k] += sx; b.ay[k] += sy; b.az[k] += sz; b.pot[k] += sp;
+                }
+            });
+        for (auto& x : th) x.join();
+    }
+    F.locals_walk = locals;
+    // L2L (translate.rs:209-252)
+    if (nthreads <= 1) {
+        l2l_down(t, locals.data(), p);
+    } else {
+        uint32_t maxl = 0;
+        for (const Cell& c : t.cells) maxl = std::max(maxl, c.level);
+        std::vector<std::vector<size_t>> lv(maxl + 1);
+        for (size_t c = 0; c < nc; ++c) lv[t.cells[c].level].push_back(c);
+        for (size_t L = 0; L <= maxl; ++L) {
+            auto& cs = lv[L];
+            std::atomic<size_t> next(0);
+            std::vector<std::thread> th;
+            for (int w = 0; w < nthreads; ++w)
+                th.emplace_back([&]() {
+                    std::vector<Cx> u(d);
+                    size_t q;
+                    while ((q = next.fetch_add(64)) < cs.size())
+                        for (size_t e = q; e < std::min(cs.size(), q + 64); ++e) {
+                            size_t c = cs[e];
+                            for (int k = 0; k < 8; ++k)
+                                if (t.cells[c].children[k] >= 0)
+                                    l2l(t, c, (size_t)t.cells[c].children[k], locals.data(), p, u.data());
+                        }
+                });
+            for (auto& x : th) x.join();
+        }
+    }
+    // L2P + scatter (translate.rs:312-407)
+    for (size_t i = 0; i < 3 * n; ++i) acc[i] = 0.0;
+    for (size_t i = 0; i < n; ++i) pot[i] = 0.0;
+    auto l2p_range = [&](size_t clo, size_t chi) {
+        std::vector<Cx> u(d);
+        for (size_t c = clo; c < chi; ++c) {
+            if (!t.cells[c].leaf) continue;
+            const Cell& cell = t.cells[c];
+            for (size_t k = cell.first; k < cell.first + cell.count; ++k) {
+                size_t id = t.order[k];
+                double p0 = 0.0;
+                double a[3] = {0.0, 0.0, 0.0};
+                double ps[3] = {b.x[k], b.y[k], b.z[k]};
+                l2p(t, c, ps, locals.data(), p, &p0, a, u.data());
+                pot[id] += b.pot[k] + p0;
+                acc[3 * id + 0] += b.ax[k] + a[0];
+                acc[3 * id + 1] += b.ay[k] + a[1];
+                acc[3 * id + 2] += b.az[k] + a[2];
+            }
+        }
+    };
+    if (nthreads <= 1) {
+        l2p_range(0, nc);
+    } else {
+        std::vector<std::thread> th;
+        for (int w = 0; w < nthreads; ++w) th.emplace_back(l2p_range, nc * w / nthreads, nc * (w + 1) / nthreads);
+        for (auto& x : th) x.join();
+    }
+    F.locals = locals;
+}
+
+}  // namespace orc
+
+// ================================================================ C interface
+using namespace orc;
+
+extern "C" {
+
+void orc_plummer(size_t n, double cx0, double cy0, double cz0, uint64_t seed, double* mass, double* pos) {
+    double c[3] = {cx0, cy0, cz0};
+    plummer(n, c, seed, mass, pos);
+}
+void orc_hernquist(size_t n, double cx0, double cy0, double cz0, uint64_t seed, double* mass, double* pos) {
+    double c[3] = {cx0, cy0, cz0};
+    hernquist(n, c, seed, mass, pos);
+}
+void orc_rng_units(uint64_t seed, size_t n, double* out) {
+    Rng r(seed);
+    for (size_t i = 0; i < n; ++i) out[i] = r.unit();
+}
+void orc_theta_table(const double* r, size_t p, double* out) { theta_table(r, p, (Cx*)out); }
+void orc_upsilon_table(const double* r, size_t p, double* out) { upsilon_table(r, p, (Cx*)out); }
+uint64_t orc_dilate(uint64_t x) { return dilate(x); }
+void orc_factorials(size_t p, double* out) {
+    auto f = factorials(p);
+    std::memcpy(out, f.data(), f.size() * sizeof(double));
+}
+void orc_binomials(size_t p, double* out) {
+    auto b = binomials(p);
+    std::memcpy(out, b.data(), b.size() * sizeof(double));
+}
+// Swap matrices B_n in block layout (rotation.rs:143-211); out has blocksum(p) entries.
+size_t orc_blocksum(size_t p) { return blocksum(p); }
+void orc_swap_matrices(size_t p, double* out) {
+    RotCtx r(p);
+    std::memcpy(out, r.sw.data(), r.sw.size() * sizeof(double));
+}
+
+// mac_mode: 0 Dehnen (reference), 1 geometric theta (extension).
+// center_mode: 0 centre of mass, 1 Ritter sphere.
+void* orc_fmm_new(size_t n, const double* pos, const double* mass, size_t p, int mac_mode, double mac_eps,
+                  double theta, double softening, size_t n_leaf, int center_mode) {
+    if (n == 0) return nullptr;  // reference panics on empty input (tree.rs:95)
+    Fmm* F = new Fmm();
+    F->p = p;
+    F->mac_mode = mac_mode;
+    F->mac_eps = mac_eps;
+    F->theta = theta;
+    F->soft2 = softening * softening;
+    build_tree(F->tree, n, pos, mass, n_leaf, center_mode);
+    return F;
+}
+void orc_fmm_refresh(void* h, size_t n, const double* pos, const double* mass) {
+    Fmm* F = (Fmm*)h;
+    build_tree(F->tree, n, pos, mass, F->tree.n_leaf, F->tree.mode);
+}
+void orc_fmm_free(void* h) { delete (Fmm*)h; }
+void orc_fmm_run(void* h, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot) {
+    run(*(Fmm*)h, n, pos, mass, nthreads, acc, pot);
+}
+size_t orc_fmm_ncells(void* h) { return ((Fmm*)h)->tree.cells.size(); }
+// Cell export: first, count, level, leaf (u32 x4 per cell), children (i32 x8),
+// cen (x3), mass, rho.
+void orc_fmm_cells(void* h, uint32_t* info, int32_t* children, double* cen, double* mass, double* rho) {
+    Fmm* F = (Fmm*)h;
+    size_t nc = F->tree.cells.size();
+    for (size_t c = 0; c < nc; ++c) {
+        const Cell& x = F->tree.cells[c];
+        info[4 * c + 0] = (uint32_t)x.first;
+        info[4 * c + 1] = (uint32_t)x.count;
+        info[4 * c + 2] = x.level;
+        info[4 * c + 3] = x.leaf ? 1u : 0u;
+        for (int k = 0; k < 8; ++k) children[8 * c + k] = x.children[k];
+        for (int d = 0; d < 3; ++d) cen[3 * c + d] = x.cen[d];
+        mass[c] = x.mass;
+        rho[c] = x.rho;
+    }
+}
+void orc_fmm_order(void* h, uint32_t* order, uint64_t* keys_sorted) {
+    Fmm* F = (Fmm*)h;
+    std::memcpy(order, F->tree.order.data(), F->tree.order.size() * 4);
+    std::memcpy(keys_sorted, F->tree.keys_sorted.data(), F->tree.keys_sorted.size() * 8);
+}
+void orc_fmm_bbox(void* h, double* out8) {
+    Fmm* F = (Fmm*)h;
+    for (int d = 0; d < 3; ++d) { out8[d] = F->tree.lo[d]; out8[3 + d] = F->tree.hi[d]; }
+    out8[6] = F->tree.side;
+    out8[7] = F->tree.inv_side;
+}
+// Intermediates of the last run.
+void orc_fmm_moments(void* h, double* out) {
+    Fmm* F = (Fmm*)h;
+    std::memcpy(out, F->moments.data(), F->moments.size() * sizeof(Cx));
+}
+void orc_fmm_locals(void* h, int after_l2l, double* out) {
+    Fmm* F = (Fmm*)h;
+    auto& v = after_l2l ? F->locals : F->locals_walk;
+    std::memcpy(out, v.data(), v.size() * sizeof(Cx));
+}
+void orc_fmm_pows(void* h, double* out) {
+    Fmm* F = (Fmm*)h;
+    std::memcpy(out, F->pows.data(), F->pows.size() * sizeof(double));
+}
+void orc_fmm_fprepass(void* h, double* f, double* fmin) {
+    Fmm* F = (Fmm*)h;
+    if (f) std::memcpy(f, F->f.data(), F->f.size() * sizeof(double));
+    if (fmin) std::memcpy(fmin, F->fmin.data(), F->fmin.size() * sizeof(double));
+}
+void orc_fmm_near(void* h, double* ax, double* ay, double* az, double* pot) {
+    Fmm* F = (Fmm*)h;
+    size_t n = F->n;
+    std::memcpy(ax, F->bodies_near.ax.data(), n * 8);
+    std::memcpy(ay, F->bodies_near.ay.data(), n * 8);
+    std::memcpy(az, F->bodies_near.az.data(), n * 8);
+    std::memcpy(pot, F->bodies_near.pot.data(), n * 8);
+}
+size_t orc_fmm_n_m2l(void* h) { return ((Fmm*)h)->lists.m2l.size() / 2; }
+size_t orc_fmm_n_p2p(void* h) { return ((Fmm*)h)->lists.p2p.size() / 2; }
+uint64_t orc_fmm_pops(void* h) { return ((Fmm*)h)->lists.pops; }
+void orc_fmm_lists(void* h, uint32_t* m2l, uint32_t* p2p) {
+    Fmm* F = (Fmm*)h;
+    if (m2l) std::memcpy(m2l, F->lists.m2l.data(), F->lists.m2l.size() * 4);
+    if (p2p) std::memcpy(p2p, F->lists.p2p.data(), F->lists.p2p.size() * 4);
+}
+
+// Kernel-level entry points used by the known-answer tests.
+// Single mutual M2L of two cells with the naive (translate.rs:47) or rotation
+// (rotation.rs:262) kernel, on given moments; locals has 2*dim entries.
+void orc_m2l_pair_test(size_t p, const double* cen_a, const double* cen_b, const double* mom_a,
+                       const double* mom_b, int use_rot, double* loc_a, double* loc_b) {
+    Tree t;
+    Cell c{};
+    for (int k = 0; k < 8; ++k) c.children[k] = -1;
+    c.leaf = true;
+    t.cells.assign(2, c);
+    for (int d = 0; d < 3; ++d) { t.cells[0].cen[d] = cen_a[d]; t.cells[1].cen[d] = cen_b[d]; }
+    size_t d = dimp(p);
+    std::vector<Cx> mom(2 * d), loc(2 * d, CZERO);
+    std::memcpy(mom.data(), mom_a, d * sizeof(Cx));
+    std::memcpy(mom.data() + d, mom_b, d * sizeof(Cx));
+    if (use_rot) {
+        RotCtx r(p);
+        r.m2l_pair(t, 0, 1, mom.data(), loc.data());
+    } else {
+        M2lScratch sc(p);
+        m2l_mutual(t, 0, 1, mom.data(), loc.data(), p, sc);
+    }
+    std::memcpy(loc_a, loc.data(), d * sizeof(Cx));
+    std::memcpy(loc_b, loc.data() + d, d * sizeof(Cx));
+}
+
+// P2P on a flat body set (slot order): self when b_first == a_first.
+void orc_p2p_test(size_t n, const double* x, const double* y, const double* z, const double* m, size_t af,
+                  size_t ac, size_t bf, size_t bc, double softening, double* ax, double* ay, double* az, double* pot) {
+    Bodies b;
+    b.x.assign(x, x + n); b.y.assign(y, y + n); b.z.assign(z, z + n); b.m.assign(m, m + n);
+    b.ax.assign(n, 0.0); b.ay.assign(n, 0.0); b.az.assign(n, 0.0); b.pot.assign(n, 0.0);
+    double s2 = softening * softening;
+    if (af == bf) p2p_self(b, af, ac, s2);
+    else p2p_pair(b, af, ac, bf, bc, s2);
+    std::memcpy(ax, b.ax.data(), n * 8); std::memcpy(ay, b.ay.data(), n * 8);
+    std::memcpy(az, b.az.data(), n * 8); std::memcpy(pot, b.pot.data(), n * 8);
+}
+
+void orc_direct(size_t n, const double* pos, const double* mass, double softening, double* acc, double* pot) {
+    direct(n, pos, mass, softening * softening, acc, pot);
+}
+void orc_direct_targets(size_t n, const double* pos, const double* mass, double softening, size_t nt,
+                        const uint32_t* tgt, double* acc, double* pot, double* f, int nthreads) {
+    direct_targets(n, pos, mass, softening * softening, nt, tgt, acc, pot, f, nthreads);
+}
+
+// scaled_error, direct.rs:35-78 -> (max_scaled, max_rel, rms_scaled, rms_rel)
+void orc_scaled_error(size_t n, const double* a_ref, const double* a_fmm, const double* pos, const double* mass,
+                      double* out4) {
+    std::vector<double> f(n, 0.0);
+    for (size_t i = 0; i < n; ++i)
+        for (size_t j = i + 1; j < n; ++j) {
+            const double* pa = &pos[3 * i];
+            const double* pb = &pos[3 * j];
+            double dx = pb[0] - pa[0], dy = pb[1] - pa[1], dz = pb[2] - pa[2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            double inv2 = 1.0 / r2;
+            f[i] += mass[j] * inv2;
+            f[j] += mass[i] * inv2;
+        }
+    double max_s = 0, max_r = 0, ss = 0, sr = 0;
+    for (size_t i = 0; i < n; ++i) {
+        double dx = a_fmm[3 * i] - a_ref[3 * i], dy = a_fmm[3 * i + 1] - a_ref[3 * i + 1],
+               dz = a_fmm[3 * i + 2] - a_ref[3 * i + 2];
+        double da = std::sqrt(dx * dx + dy * dy + dz * dz);
+        double ar = std::sqrt(a_ref[3 * i] * a_ref[3 * i] + a_ref[3 * i + 1] * a_ref[3 * i + 1] +
+                              a_ref[3 * i + 2] * a_ref[3 * i + 2]);
+        double s = da / f[i];
+        double rel = ar > 0.0 ? da / ar : 0.0;
+        max_s = fmax_rs(max_s, s);
+        max_r = fmax_rs(max_r, rel);
+        ss += s * s;
+        sr += rel * rel;
+    }
+    out4[0] = max_s;
+    out4[1] = max_r;
+    out4[2] = std::sqrt(ss / (double)n);
+    out4[3] = std::sqrt(sr / (double)n);
+}
+
+// Sampled targets of crates/bench/src/main.rs:34-78 (LCG, seed given).
+void orc_sample_targets(size_t n, uint64_t seed, size_t samp, uint32_t* out) {
+    uint64_t rng = seed;
+    for (size_t q = 0; q < samp; ++q) {
+        rng = rng * 6364136223846793005ULL + 1442695040888963407ULL;
+        out[q] = (uint32_t)((rng >> 33) % n);
+    }
+}
+
+}  // extern "C"
