@@ -1,0 +1,894 @@
+// Host orchestration of the engine behind the C ABI (include/fmmx.h).
+//
+// fmmx_build   = Fmm::new / refresh (fmm.rs:26-56): bounding box, Morton keys,
+//                key sort, level-by-level node creation, depth-first
+//                renumbering, body gather, cell geometry.
+// fmmx_evaluate = Fmm::run (fmm.rs:60-142): gather, f pre-pass, P2M/M2M and
+//                multipole power, dual walk, directed lists, M2L, L2L, P2P,
+//                L2P + scatter.
+//
+// All work runs on one stream; the host waits on it only where a size must be
+// known (node count after the build, list lengths after the walk).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "sort.h"
+
+using namespace fmmx;
+
+namespace {
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        release();
+        size_t want = std::max<size_t>(n, 1);
+        cudaError_t e = cudaMalloc((void**)&p, want * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return e;
+        }
+        cap = want;
+        return cudaSuccess;
+    }
+};
+
+int bits_for(uint64_t v) {
+    int b = 0;
+    while (b < 64 && (v >> b) != 0) ++b;
+    return std::max(b, 1);
+}
+
+struct Status {
+    fmmx_status code = FMMX_OK;
+    std::string msg;
+};
+
+}  // namespace
+
+struct fmmx_ctx {
+    fmmx_config cfg;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    OrderTables tab;
+    std::vector<double> swap_host;
+    DBuf<double> swap_dev;
+
+    // sizes of the current tree
+    size_t n = 0;
+    int nc = 0, nleaves = 0, nlevels = 0;
+    int lvl_start[FMMX_NLEVELS + 1] = {0}, lvl_count[FMMX_NLEVELS + 1] = {0};
+    bool built = false, evaluated = false;
+    int n_m2l = 0, n_p2p = 0;
+    unsigned long long pops = 0, p2p_inter = 0;
+
+    // inputs (host API copies) and outputs
+    DBuf<double> pos_in, mass_in, acc_out, pot_out;
+    const double* build_pos = nullptr;  // device pointers of the last build's inputs
+    const double* build_mass = nullptr;
+
+    DBuf<double> box, bbox_part;
+    DBuf<int> flags;
+    DBuf<uint64_t> keys, keys_sorted;
+    DBuf<uint32_t> idx, order;
+    DBuf<double> x, y, z, m, nax, nay, naz, npot;
+    DBuf<char> cub_tmp;
+
+    // nodes before renumbering
+    DBuf<uint32_t> t_first, t_count;
+    DBuf<int32_t> t_parent;
+    DBuf<uint8_t> t_oct, t_level, t_leaf;
+    uint32_t tcap = 0;
+    DBuf<int> lvl;
+    DBuf<uint64_t> dfs_key, dfs_key_alt;
+    DBuf<uint32_t> dfs_val, dfs_val_alt;
+    DBuf<int32_t> new_id;
+
+    // cells (depth-first pre-order)
+    DBuf<uint32_t> c_first, c_count;
+    DBuf<int32_t> c_child, c_parent, level_cells, body_leaf;
+    DBuf<uint8_t> c_leaf, c_level;
+    DBuf<double> c_cx, c_cy, c_cz, c_mass, c_rho;
+
+    // expansions
+    DBuf<zd> moments, locals;
+    DBuf<double> pows, f, fmin;
+
+    // walk
+    DBuf<uint2> front0, front1, m2l, p2p;
+    DBuf<int> wcounts;
+    DBuf<unsigned long long> wpops, inter;
+    uint32_t cap_front = 0, cap_m2l = 0, cap_p2p = 0;
+
+    // directed lists
+    DBuf<uint64_t> m2l_keys, m2l_keys_s, p2p_keys, p2p_keys_s;
+    DBuf<uint32_t> m2l_seg_b, m2l_seg_e, p2p_seg_b, p2p_seg_e;
+
+    fmmx_stats st;
+    cudaEvent_t ev[12];
+    bool events = false;
+};
+
+namespace {
+
+fmmx_status fail(fmmx_ctx* c, fmmx_status s, const std::string& msg) {
+    c->err = msg;
+    return s;
+}
+
+fmmx_status cuda_fail(fmmx_ctx* c, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation) return fail(c, FMMX_OUT_OF_MEMORY, m);
+    return fail(c, FMMX_DEVICE_ERROR, m);
+}
+
+#define CK(expr, where)                                   \
+    do {                                                  \
+        cudaError_t e__ = (expr);                         \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, where); \
+    } while (0)
+
+#define CKL(where) CK(cudaGetLastError(), where)
+
+CellsView view(fmmx_ctx* c) {
+    CellsView v;
+    v.first = c->c_first.p;
+    v.count = c->c_count.p;
+    v.child = c->c_child.p;
+    v.leaf = c->c_leaf.p;
+    v.level = c->c_level.p;
+    v.cx = c->c_cx.p;
+    v.cy = c->c_cy.p;
+    v.cz = c->c_cz.p;
+    v.mass = c->c_mass.p;
+    v.rho = c->c_rho.p;
+    return v;
+}
+
+CellsMut view_mut(fmmx_ctx* c) {
+    CellsMut v;
+    v.first = c->c_first.p;
+    v.count = c->c_count.p;
+    v.child = c->c_child.p;
+    v.parent = c->c_parent.p;
+    v.leaf = c->c_leaf.p;
+    v.level = c->c_level.p;
+    v.cx = c->c_cx.p;
+    v.cy = c->c_cy.p;
+    v.cz = c->c_cz.p;
+    v.mass = c->c_mass.p;
+    v.rho = c->c_rho.p;
+    return v;
+}
+
+// Swap matrices B_n in block layout, Dehnen 2014 eq 63 (rotation.rs:136-211).
+void build_swap(int p, std::vector<double>& sw) {
+    auto boff = [](int j) { return j == 0 ? 0 : j * (4 * j * j - 1) / 3; };
+    const int bs = (p + 1) * (4 * p * p + 8 * p + 3) / 3;
+    sw.assign(bs, 0.0);
+    sw[0] = 1.0;
+    for (int n = 1; n <= p; ++n) {
+        const int nb = 2 * n + 1, off = boff(n), nbp = 2 * n - 1, offp = boff(n - 1);
+        auto prev = [&](int row_base, int l) -> double {
+            return (std::abs(l) <= n - 1) ? sw[row_base + l + (n - 1)] : 0.0;
+        };
+        for (int mr = 0; mr < nb; ++mr) {
+            const int mm = mr - n;
+            for (int lc = 0; lc < nb; ++lc) {
+                const int l = lc - n;
+                double v;
+                if (std::abs(mm) <= n - 1) {
+                    const int rp = offp + (mr - 1) * nbp;
+                    v = (prev(rp, l - 1) - prev(rp, l + 1)) * 0.5;
+                } else if (mm == n) {
+                    const int src = offp + (2 * n - 2) * nbp;
+                    v = (prev(src, l - 1) + prev(src, l + 1) + 2.0 * prev(src, l)) * 0.5;
+                } else {
+                    const int src = offp;
+                    v = (prev(src, l - 1) + prev(src, l + 1) - 2.0 * prev(src, l)) * 0.5;
+                }
+                sw[off + mr * nb + lc] = v;
+            }
+        }
+    }
+}
+
+void make_tables(int p, OrderTables& t) {
+    std::memset(&t, 0, sizeof(t));
+    t.fact[0] = 1.0;
+    for (int i = 1; i <= 2 * p; ++i) t.fact[i] = t.fact[i - 1] * (double)i;  // moments.rs:11-17
+    for (int k = 0; k <= p; ++k) t.binom[k] = t.fact[p] / (t.fact[k] * t.fact[p - k]);  // :20-27
+    for (int m = 1; m <= p; ++m) t.inv2m[m] = 1.0 / (double)(2 * m);
+    for (int n = 0; n <= p; ++n)
+        for (int m = 0; m < n; ++m) t.invc[n][m] = 1.0 / (double)(n * n - m * m);
+}
+
+bool use_rotation(const fmmx_config& c) {
+    if (c.m2l_kernel == FMMX_M2L_ROTATION) return true;
+    if (c.m2l_kernel == FMMX_M2L_NAIVE) return false;
+    return c.p >= 20;  // rotation.rs:45 ROT_P
+}
+
+const unsigned kGrid = 148u * 8u;
+
+// ---------------------------------------------------------------- build
+fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const double* d_mass) {
+    cudaStream_t s = ctx->stream;
+    if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input (the reference asserts !parts.is_empty(), tree.rs:95)");
+    if (n >= (1ull << 31)) return fail(ctx, FMMX_INVALID_ARG, "n must be below 2^31");
+    ctx->built = false;
+    ctx->evaluated = false;
+    ctx->n = n;
+    if (ctx->events) CK(cudaEventRecord(ctx->ev[0], s), "event");
+    CK(ctx->keys.ensure(n), "alloc keys");
+    CK(ctx->keys_sorted.ensure(n), "alloc keys");
+    CK(ctx->idx.ensure(n), "alloc idx");
+    CK(ctx->order.ensure(n), "alloc order");
+    for (DBuf<double>* b : {&ctx->x, &ctx->y, &ctx->z, &ctx->m, &ctx->nax, &ctx->nay, &ctx->naz, &ctx->npot})
+        CK(b->ensure(n), "alloc bodies");
+    CK(ctx->box.ensure(8), "alloc box");
+    const unsigned gb = std::min<unsigned>(grid_for(n, 256), 1024u);
+    CK(ctx->bbox_part.ensure(gb * 6), "alloc box");
+    CK(ctx->flags.ensure(8), "alloc flags");
+    CK(cudaMemsetAsync(ctx->flags.p, 0, 8 * sizeof(int), s), "memset");
+
+    k_bbox_partial<<<gb, 256, 0, s>>>(d_pos, n, ctx->bbox_part.p, ctx->flags.p + 2);
+    k_bbox_final<<<1, 32, 0, s>>>(ctx->bbox_part.p, (int)gb, ctx->box.p);
+    k_keys<<<grid_for(n, 256), 256, 0, s>>>(d_pos, n, ctx->box.p, ctx->keys.p, ctx->idx.p);
+    CKL("keys");
+    const int nbits = 3 * FMMX_BITS;
+    size_t tb = sort_pairs_u64_u32_temp((int)n, nbits);
+    CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+    CK(sort_pairs_u64_u32(ctx->cub_tmp.p, tb, ctx->keys.p, ctx->keys_sorted.p, ctx->idx.p, ctx->order.p, (int)n, nbits,
+                          s),
+       "key sort");
+    k_gather<<<grid_for(n, 256), 256, 0, s>>>(d_pos, d_mass, ctx->order.p, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p);
+    CKL("gather");
+
+    // level-by-level node creation, retried with more room on overflow
+    CK(ctx->lvl.ensure(LV_SIZE), "alloc lvl");
+    if (ctx->tcap == 0) {
+        uint64_t est = 4ull * n / (uint64_t)std::max(ctx->cfg.n_leaf, 1) + 8ull * FMMX_NLEVELS + 64;
+        ctx->tcap = (uint32_t)std::min<uint64_t>(est, 0x7fffffffull);
+    }
+    int hl[LV_SIZE];
+    int hflags[8];
+    for (int attempt = 0;; ++attempt) {
+        const uint32_t cap = ctx->tcap;
+        CK(ctx->t_first.ensure(cap), "alloc nodes");
+        CK(ctx->t_count.ensure(cap), "alloc nodes");
+        CK(ctx->t_parent.ensure(cap), "alloc nodes");
+        CK(ctx->t_oct.ensure(cap), "alloc nodes");
+        CK(ctx->t_level.ensure(cap), "alloc nodes");
+        CK(ctx->t_leaf.ensure(cap), "alloc nodes");
+        TmpNodes tn{ctx->t_first.p, ctx->t_count.p, ctx->t_parent.p, ctx->t_oct.p, ctx->t_level.p, ctx->t_leaf.p};
+        CK(cudaMemsetAsync(ctx->lvl.p, 0, LV_SIZE * sizeof(int), s), "memset");
+        CK(cudaMemsetAsync(ctx->flags.p, 0, 2 * sizeof(int), s), "memset");
+        k_tree_init<<<1, 32, 0, s>>>(tn, (uint32_t)n, ctx->lvl.p);
+        const unsigned gl = std::min<unsigned>(grid_for(cap, 256), kGrid);
+        for (int L = 0; L < FMMX_NLEVELS; ++L)
+            k_build_level<<<gl, 256, 0, s>>>(tn, ctx->keys_sorted.p, L, (long long)ctx->cfg.n_leaf, cap, ctx->lvl.p,
+                                              ctx->flags.p);
+        CKL("build levels");
+        CK(cudaMemcpyAsync(hl, ctx->lvl.p, sizeof(hl), cudaMemcpyDeviceToHost, s), "copy");
+        CK(cudaMemcpyAsync(hflags, ctx->flags.p, sizeof(hflags), cudaMemcpyDeviceToHost, s), "copy");
+        CK(cudaStreamSynchronize(s), "tree build");
+        if (hflags[2]) return fail(ctx, FMMX_INVALID_ARG, "non-finite position");
+        if (!hflags[0]) break;
+        uint64_t total = 0;
+        for (int L = 0; L < FMMX_NLEVELS; ++L) total += (uint64_t)hl[LV_COUNT + L];
+        uint64_t want = std::max<uint64_t>(2ull * cap, total + total / 2 + 64);
+        if (want > 0x7fffffffull || attempt > 8) return fail(ctx, FMMX_OUT_OF_MEMORY, "node capacity");
+        ctx->tcap = (uint32_t)want;
+    }
+    int nc = 0, nlev = 0;
+    for (int L = 0; L < FMMX_NLEVELS; ++L) {
+        ctx->lvl_start[L] = nc;
+        ctx->lvl_count[L] = hl[LV_COUNT + L];
+        nc += hl[LV_COUNT + L];
+        if (hl[LV_COUNT + L] > 0) nlev = L + 1;
+    }
+    ctx->nc = nc;
+    ctx->nlevels = nlev;
+    ctx->nleaves = hflags[1];
+
+    // depth-first renumbering: sort nodes by (first slot, level)
+    TmpNodes tn{ctx->t_first.p, ctx->t_count.p, ctx->t_parent.p, ctx->t_oct.p, ctx->t_level.p, ctx->t_leaf.p};
+    CK(ctx->dfs_key.ensure(nc), "alloc");
+    CK(ctx->dfs_key_alt.ensure(nc), "alloc");
+    CK(ctx->dfs_val.ensure(nc), "alloc");
+    CK(ctx->dfs_val_alt.ensure(nc), "alloc");
+    CK(ctx->new_id.ensure(nc), "alloc");
+    k_dfs_keys<<<grid_for(nc, 256), 256, 0, s>>>(tn, nc, ctx->dfs_key.p, ctx->dfs_val.p);
+    const int dbits = 5 + bits_for(n);
+    tb = sort_pairs_u64_u32_temp(nc, dbits);
+    CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+    CK(sort_pairs_u64_u32(ctx->cub_tmp.p, tb, ctx->dfs_key.p, ctx->dfs_key_alt.p, ctx->dfs_val.p, ctx->dfs_val_alt.p,
+                          nc, dbits, s),
+       "dfs sort");
+    for (DBuf<uint32_t>* b : {&ctx->c_first, &ctx->c_count}) CK(b->ensure(nc), "alloc cells");
+    CK(ctx->c_child.ensure(8 * (size_t)nc), "alloc cells");
+    CK(ctx->c_parent.ensure(nc), "alloc cells");
+    CK(ctx->level_cells.ensure(nc), "alloc cells");
+    CK(ctx->body_leaf.ensure(n), "alloc cells");
+    CK(ctx->c_leaf.ensure(nc), "alloc cells");
+    CK(ctx->c_level.ensure(nc), "alloc cells");
+    for (DBuf<double>* b : {&ctx->c_cx, &ctx->c_cy, &ctx->c_cz, &ctx->c_mass, &ctx->c_rho})
+        CK(b->ensure(nc), "alloc cells");
+    CK(cudaMemsetAsync(ctx->c_child.p, 0xff, 8 * (size_t)nc * sizeof(int32_t), s), "memset");
+    k_finalize_cells<<<grid_for(nc, 256), 256, 0, s>>>(ctx->dfs_val_alt.p, nc, tn, ctx->new_id.p, view_mut(ctx));
+    k_link_cells<<<grid_for(nc, 256), 256, 0, s>>>(nc, tn, ctx->new_id.p, view_mut(ctx), ctx->level_cells.p);
+    k_body_leaf<<<grid_for((size_t)nc * 32, 256), 256, 0, s>>>(nc, ctx->c_first.p, ctx->c_count.p, ctx->c_leaf.p,
+                                                               ctx->body_leaf.p);
+    CKL("finalize cells");
+    for (int L = nlev - 1; L >= 0; --L) {
+        const int cnt = ctx->lvl_count[L];
+        k_geometry_level<<<grid_for(cnt, 128), 128, 0, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt,
+                                                            view_mut(ctx), ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p,
+                                                            ctx->cfg.center_mode);
+    }
+    CKL("geometry");
+    if (ctx->events) CK(cudaEventRecord(ctx->ev[1], s), "event");
+    CK(cudaStreamSynchronize(s), "build");
+    if (ctx->events) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+        ctx->st.ms_build = ms;
+    }
+    ctx->build_pos = d_pos;
+    ctx->build_mass = d_mass;
+    ctx->built = true;
+    return FMMX_OK;
+}
+
+// ---------------------------------------------------------------- evaluate
+fmmx_status walk_impl(fmmx_ctx* ctx) {
+    cudaStream_t s = ctx->stream;
+    const int nc = ctx->nc;
+    if (ctx->cap_front == 0) {
+        ctx->cap_front = (uint32_t)std::min<uint64_t>(64ull * nc + 1024, 0x7fffffffull);
+        ctx->cap_m2l = (uint32_t)std::min<uint64_t>(64ull * nc + 1024, 0x7fffffffull);
+        ctx->cap_p2p = (uint32_t)std::min<uint64_t>(32ull * nc + 1024, 0x7fffffffull);
+    }
+    CK(ctx->wcounts.ensure(WC_SIZE), "alloc");
+    CK(ctx->wpops.ensure(1), "alloc");
+    MacParams mp;
+    mp.mode = ctx->cfg.mac_mode;
+    mp.p = ctx->cfg.p;
+    mp.eps = ctx->cfg.mac_eps;
+    mp.theta = ctx->cfg.theta;
+    const CellsView cv = view(ctx);
+    for (int attempt = 0;; ++attempt) {
+        CK(ctx->front0.ensure(ctx->cap_front), "alloc walk");
+        CK(ctx->front1.ensure(ctx->cap_front), "alloc walk");
+        CK(ctx->m2l.ensure(ctx->cap_m2l), "alloc walk");
+        CK(ctx->p2p.ensure(ctx->cap_p2p), "alloc walk");
+        WalkBufs w;
+        w.front[0] = ctx->front0.p;
+        w.front[1] = ctx->front1.p;
+        w.m2l = ctx->m2l.p;
+        w.p2p = ctx->p2p.p;
+        w.counts = ctx->wcounts.p;
+        w.pops_ptr = ctx->wpops.p;
+        w.cap_front = ctx->cap_front;
+        w.cap_m2l = ctx->cap_m2l;
+        w.cap_p2p = ctx->cap_p2p;
+        CK(cudaMemsetAsync(ctx->wcounts.p, 0, WC_SIZE * sizeof(int), s), "memset");
+        CK(cudaMemsetAsync(ctx->wpops.p, 0, sizeof(unsigned long long), s), "memset");
+        CK(cudaMemsetAsync(ctx->front0.p, 0, sizeof(uint2), s), "memset");  // root pair (0, 0)
+        const int one = 1;
+        CK(cudaMemcpyAsync(ctx->wcounts.p + WC_FRONT0, &one, sizeof(int), cudaMemcpyHostToDevice, s), "copy");
+        int cur = 0;
+        int hc[WC_SIZE];
+        bool done = false;
+        const int max_iter = 8 * FMMX_NLEVELS + 16;
+        for (int it = 0; it < max_iter && !done;) {
+            for (int b = 0; b < 6; ++b, ++it) {
+                k_walk_iter<<<kGrid, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
+                CK(cudaMemsetAsync(ctx->wcounts.p + cur, 0, sizeof(int), s), "memset");
+                cur ^= 1;
+            }
+            CKL("walk");
+            CK(cudaMemcpyAsync(hc, ctx->wcounts.p, sizeof(hc), cudaMemcpyDeviceToHost, s), "copy");
+            CK(cudaStreamSynchronize(s), "walk");
+            if (hc[WC_OVERFLOW] || hc[cur] == 0) done = true;
+        }
+        if (!done) return fail(ctx, FMMX_TIMEOUT, "dual walk did not terminate");
+        if (hc[WC_OVERFLOW]) {
+            if (attempt > 8) return fail(ctx, FMMX_OUT_OF_MEMORY, "walk capacity");
+            auto grow = [](uint32_t c, int used) {
+                uint64_t w2 = std::max<uint64_t>(2ull * c, (uint64_t)used + (uint64_t)used / 2 + 1024);
+                return (uint32_t)std::min<uint64_t>(w2, 0x7fffffffull);
+            };
+            if (hc[WC_OVERFLOW] & 1) ctx->cap_front = grow(ctx->cap_front, 0);
+            if (hc[WC_OVERFLOW] & 2) ctx->cap_p2p = grow(ctx->cap_p2p, hc[WC_P2P]);
+            if (hc[WC_OVERFLOW] & 4) ctx->cap_m2l = grow(ctx->cap_m2l, hc[WC_M2L]);
+            continue;
+        }
+        ctx->n_m2l = hc[WC_M2L];
+        ctx->n_p2p = hc[WC_P2P];
+        CK(cudaMemcpy(&ctx->pops, ctx->wpops.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "copy");
+        return FMMX_OK;
+    }
+}
+
+fmmx_status lists_impl(fmmx_ctx* ctx) {
+    cudaStream_t s = ctx->stream;
+    const int nc = ctx->nc;
+    const int cbits = 32 + bits_for((uint64_t)nc);
+    // M2L
+    const int nm = ctx->n_m2l;
+    CK(ctx->m2l_seg_b.ensure(nc), "alloc lists");
+    CK(ctx->m2l_seg_e.ensure(nc), "alloc lists");
+    CK(cudaMemsetAsync(ctx->m2l_seg_b.p, 0, nc * sizeof(uint32_t), s), "memset");
+    CK(cudaMemsetAsync(ctx->m2l_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
+    if (nm > 0) {
+        CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
+        CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
+        k_expand_m2l<<<grid_for(nm, 256), 256, 0, s>>>(ctx->m2l.p, nm, ctx->m2l_keys.p);
+        size_t tb = sort_keys_u64_temp(2 * nm, cbits);
+        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+        CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
+        k_segments<<<grid_for(2 * (size_t)nm, 256), 256, 0, s>>>(ctx->m2l_keys_s.p, 2 * nm, ctx->m2l_seg_b.p,
+                                                                 ctx->m2l_seg_e.p);
+        CKL("m2l lists");
+    }
+    // P2P
+    const int np = ctx->n_p2p;
+    CK(ctx->p2p_seg_b.ensure(nc), "alloc lists");
+    CK(ctx->p2p_seg_e.ensure(nc), "alloc lists");
+    CK(ctx->inter.ensure(1), "alloc");
+    CK(cudaMemsetAsync(ctx->p2p_seg_b.p, 0, nc * sizeof(uint32_t), s), "memset");
+    CK(cudaMemsetAsync(ctx->p2p_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
+    CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
+    if (np > 0) {
+        CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
+        CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
+        const uint64_t sentinel = (uint64_t)nc << 32;
+        k_expand_p2p<<<grid_for(np, 256), 256, 0, s>>>(ctx->p2p.p, np, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
+                                                       ctx->inter.p);
+        size_t tb = sort_keys_u64_temp(2 * np, cbits);
+        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+        CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->p2p_keys.p, ctx->p2p_keys_s.p, 2 * np, cbits, s), "p2p sort");
+        const int nvalid = 2 * np - ctx->nleaves;
+        k_segments<<<grid_for(nvalid, 256), 256, 0, s>>>(ctx->p2p_keys_s.p, nvalid, ctx->p2p_seg_b.p,
+                                                         ctx->p2p_seg_e.p);
+        CKL("p2p lists");
+    }
+    return FMMX_OK;
+}
+
+fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+    cudaStream_t s = ctx->stream;
+    if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
+    const int p = ctx->cfg.p, dim = dimp(p), nc = ctx->nc;
+    const size_t n = ctx->n;
+    cudaEvent_t* ev = ctx->ev;
+    const bool tm = ctx->events;
+    if (tm) CK(cudaEventRecord(ev[2], s), "event");
+    if (d_pos == nullptr) d_pos = ctx->build_pos;
+    if (d_mass == nullptr) d_mass = ctx->build_mass;
+    k_gather<<<grid_for(n, 256), 256, 0, s>>>(d_pos, d_mass, ctx->order.p, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p);
+    CKL("gather");
+    CK(ctx->moments.ensure((size_t)nc * dim), "alloc expansions");
+    CK(ctx->locals.ensure((size_t)nc * dim), "alloc expansions");
+    CK(ctx->pows.ensure((size_t)nc * (p + 1)), "alloc expansions");
+    CK(ctx->fmin.ensure(nc), "alloc expansions");
+    CK(ctx->f.ensure(n), "alloc expansions");
+    const bool dehnen = ctx->cfg.mac_mode == FMMX_MAC_DEHNEN;
+    const CellsView cv = view(ctx);
+    if (dehnen) {
+        CK(cudaMemsetAsync(ctx->flags.p + 3, 0, sizeof(int), s), "memset");
+        k_fprepass<<<grid_for(n, 128), 128, 0, s>>>(cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, n, ctx->f.p,
+                                                    ctx->flags.p + 3);
+        CKL("f pre-pass");
+    }
+    {
+        const int warps = 4;
+        const size_t smem = (size_t)warps * 2 * dim * sizeof(zd);
+        if (smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_upward_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+        for (int L = ctx->nlevels - 1; L >= 0; --L) {
+            const int cnt = ctx->lvl_count[L];
+            unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, kGrid);
+            k_upward_exact<<<g, 32 * warps, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->x.p,
+                                                       ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->moments.p, ctx->pows.p,
+                                                       dehnen ? ctx->f.p : nullptr, ctx->fmin.p);
+        }
+        CKL("upward");
+    }
+    if (tm) CK(cudaEventRecord(ev[3], s), "event");
+    fmmx_status st = walk_impl(ctx);
+    if (st != FMMX_OK) return st;
+    if (dehnen) {
+        int bad = 0;
+        CK(cudaMemcpy(&bad, ctx->flags.p + 3, sizeof(int), cudaMemcpyDeviceToHost), "copy");
+        if (bad) return fail(ctx, FMMX_DEVICE_ERROR, "f pre-pass stack overflow");
+    }
+    if (tm) CK(cudaEventRecord(ev[4], s), "event");
+    st = lists_impl(ctx);
+    if (st != FMMX_OK) return st;
+    if (tm) CK(cudaEventRecord(ev[5], s), "event");
+
+    DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p};
+    DirList lp{ctx->p2p_keys_s.p, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p};
+    CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
+    if (ctx->n_m2l > 0) {
+        const unsigned g = std::min<unsigned>(nc, 148u * 16u);
+        if (use_rotation(ctx->cfg)) {
+            const size_t smem = m2l_rot_smem_bytes(p);
+            CK(cudaFuncSetAttribute(k_m2l_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+            k_m2l_rot_f64<<<g, 128, smem, s>>>(lm, nc, cv, p, ctx->moments.p, ctx->locals.p, ctx->swap_dev.p);
+        } else {
+            const size_t smem = 2 * (size_t)dim * sizeof(zd);
+            k_m2l_naive_f64<<<g, 128, smem, s>>>(lm, nc, cv, p, ctx->moments.p, ctx->locals.p);
+        }
+        CKL("m2l");
+    }
+    if (tm) CK(cudaEventRecord(ev[6], s), "event");
+    {
+        const size_t smem = 2 * (size_t)dim * sizeof(zd);
+        for (int L = 1; L < ctx->nlevels; ++L) {
+            const int cnt = ctx->lvl_count[L];
+            k_l2l_f64<<<std::min<unsigned>(cnt, 148u * 16u), 128, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L],
+                                                                            cnt, cv, ctx->c_parent.p, p,
+                                                                            ctx->locals.p);
+        }
+        CKL("l2l");
+    }
+    if (tm) CK(cudaEventRecord(ev[7], s), "event");
+    {
+        const double soft2 = ctx->cfg.softening * ctx->cfg.softening;
+        k_p2p_f64<<<std::min<unsigned>(nc, 148u * 16u), 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
+                                                                      ctx->m.p, soft2, ctx->nax.p, ctx->nay.p,
+                                                                      ctx->naz.p, ctx->npot.p);
+        CKL("p2p");
+    }
+    if (tm) CK(cudaEventRecord(ev[8], s), "event");
+    k_l2p_f64<<<grid_for(n, 128), 128, 0, s>>>(n, ctx->body_leaf.p, ctx->order.p, cv, p, ctx->locals.p, ctx->x.p,
+                                               ctx->y.p, ctx->z.p, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p,
+                                               d_acc, d_pot);
+    CKL("l2p");
+    if (tm) CK(cudaEventRecord(ev[9], s), "event");
+    CK(cudaStreamSynchronize(s), "evaluate");
+    CK(cudaMemcpy(&ctx->p2p_inter, ctx->inter.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "copy");
+    if (tm) {
+        auto el = [&](int a, int b) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[a], ev[b]);
+            return (double)ms;
+        };
+        ctx->st.ms_upward = el(2, 3);
+        ctx->st.ms_walk = el(3, 4);
+        ctx->st.ms_lists = el(4, 5);
+        ctx->st.ms_m2l = el(5, 6);
+        ctx->st.ms_l2l = el(6, 7);
+        ctx->st.ms_p2p = el(7, 8);
+        ctx->st.ms_l2p = el(8, 9);
+        ctx->st.ms_evaluate = el(2, 9);
+    }
+    ctx->evaluated = true;
+    return FMMX_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+void fmmx_config_default(fmmx_config* c) {
+    if (!c) return;
+    c->p = 8;
+    c->mac_mode = FMMX_MAC_DEHNEN;
+    c->mac_eps = 1e-5;
+    c->theta = 0.5;
+    c->softening = 0.0;
+    c->n_leaf = 16;
+    c->center_mode = FMMX_CENTER_COM;
+    c->precision = FMMX_PLAIN_FP64;
+    c->m2l_kernel = FMMX_M2L_AUTO;
+    c->device = 0;
+    c->stream = nullptr;
+}
+
+const char* fmmx_status_string(fmmx_status s) {
+    switch (s) {
+        case FMMX_OK: return "ok";
+        case FMMX_INVALID_ARG: return "invalid argument";
+        case FMMX_OUT_OF_MEMORY: return "out of memory";
+        case FMMX_OVER_BUDGET: return "over budget";
+        case FMMX_LEAF_OVERFLOW: return "leaf overflow";
+        case FMMX_DEVICE_ERROR: return "device error";
+        case FMMX_TIMEOUT: return "timeout";
+        case FMMX_NOT_BUILT: return "not built";
+        case FMMX_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown";
+}
+
+fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
+    if (!out) return FMMX_INVALID_ARG;
+    *out = nullptr;
+    fmmx_config c;
+    if (cfg) c = *cfg;
+    else fmmx_config_default(&c);
+    if (c.p < 1 || c.p > FMMX_MAXP) return FMMX_INVALID_ARG;
+    if (c.n_leaf < 0) return FMMX_INVALID_ARG;
+    if (c.mac_mode != FMMX_MAC_DEHNEN && c.mac_mode != FMMX_MAC_THETA) return FMMX_INVALID_ARG;
+    if (c.mac_mode == FMMX_MAC_THETA && !(c.theta > 0.0)) return FMMX_INVALID_ARG;
+    if (!(c.softening >= 0.0)) return FMMX_INVALID_ARG;
+    if (c.center_mode != FMMX_CENTER_COM && c.center_mode != FMMX_CENTER_SPHERE) return FMMX_INVALID_ARG;
+    if (c.precision != FMMX_PLAIN_FP64 && c.precision != FMMX_MIXED) return FMMX_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FMMX_NO_DEVICE;
+    }
+    if (c.device < 0 || c.device >= ndev) return FMMX_INVALID_ARG;
+    if (cudaSetDevice(c.device) != cudaSuccess) return FMMX_DEVICE_ERROR;
+    fmmx_ctx* ctx = new fmmx_ctx();
+    ctx->cfg = c;
+    std::memset(&ctx->st, 0, sizeof(ctx->st));
+    if (c.stream) {
+        ctx->stream = (cudaStream_t)c.stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return FMMX_DEVICE_ERROR;
+        }
+        ctx->own_stream = true;
+    }
+    ctx->events = true;
+    for (int i = 0; i < 12; ++i) cudaEventCreate(&ctx->ev[i]);
+    make_tables(c.p, ctx->tab);
+    upload_tables_exact(ctx->tab, ctx->stream);
+    upload_tables_m2l(ctx->tab, ctx->stream);
+    upload_tables_sweeps(ctx->tab, ctx->stream);
+    build_swap(c.p, ctx->swap_host);
+    if (ctx->swap_dev.ensure(ctx->swap_host.size()) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->swap_dev.p, ctx->swap_host.data(), ctx->swap_host.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        fmmx_destroy(ctx);
+        return FMMX_DEVICE_ERROR;
+    }
+    *out = ctx;
+    return FMMX_OK;
+}
+
+void fmmx_destroy(fmmx_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->cfg.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < 12; ++i)
+        if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* fmmx_last_error(const fmmx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+fmmx_status fmmx_build_device(fmmx_ctx* ctx, size_t n, const double* d_pos, const double* d_mass) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!d_pos || !d_mass) return fail(ctx, FMMX_INVALID_ARG, "null input");
+    cudaSetDevice(ctx->cfg.device);
+    return build_impl(ctx, n, d_pos, d_mass);
+}
+
+fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double* mass) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!pos || !mass) return fail(ctx, FMMX_INVALID_ARG, "null input");
+    if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input (the reference asserts !parts.is_empty(), tree.rs:95)");
+    cudaSetDevice(ctx->cfg.device);
+    if (ctx->pos_in.ensure(3 * n) != cudaSuccess || ctx->mass_in.ensure(n) != cudaSuccess)
+        return fail(ctx, FMMX_OUT_OF_MEMORY, "input buffers");
+    cudaStream_t s = ctx->stream;
+    if (cudaMemcpyAsync(ctx->pos_in.p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->mass_in.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
+    return build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p);
+}
+
+fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc,
+                                 double* d_pot) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!d_acc) return fail(ctx, FMMX_INVALID_ARG, "null output");
+    cudaSetDevice(ctx->cfg.device);
+    if (!d_pot) {
+        if (ctx->pot_out.ensure(ctx->n) != cudaSuccess) return fail(ctx, FMMX_OUT_OF_MEMORY, "pot buffer");
+        d_pot = ctx->pot_out.p;
+    }
+    return evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot);
+}
+
+fmmx_status fmmx_evaluate(fmmx_ctx* ctx, const double* pos, const double* mass, double* acc, double* pot) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!acc) return fail(ctx, FMMX_INVALID_ARG, "null output");
+    if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
+    cudaSetDevice(ctx->cfg.device);
+    const size_t n = ctx->n;
+    cudaStream_t s = ctx->stream;
+    const double* dp = nullptr;
+    const double* dm = nullptr;
+    if (pos || mass) {
+        if (ctx->pos_in.ensure(3 * n) != cudaSuccess || ctx->mass_in.ensure(n) != cudaSuccess)
+            return fail(ctx, FMMX_OUT_OF_MEMORY, "input buffers");
+        if (pos) {
+            if (cudaMemcpyAsync(ctx->pos_in.p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+                return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
+            dp = ctx->pos_in.p;
+        }
+        if (mass) {
+            if (cudaMemcpyAsync(ctx->mass_in.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+                return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
+            dm = ctx->mass_in.p;
+        }
+    }
+    if (ctx->acc_out.ensure(3 * n) != cudaSuccess || ctx->pot_out.ensure(n) != cudaSuccess)
+        return fail(ctx, FMMX_OUT_OF_MEMORY, "output buffers");
+    fmmx_status st = evaluate_impl(ctx, dp, dm, ctx->acc_out.p, ctx->pot_out.p);
+    if (st != FMMX_OK) return st;
+    if (cudaMemcpyAsync(acc, ctx->acc_out.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return cuda_fail(ctx, cudaGetLastError(), "copy outputs");
+    if (pot && cudaMemcpyAsync(pot, ctx->pot_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return cuda_fail(ctx, cudaGetLastError(), "copy outputs");
+    if (cudaStreamSynchronize(s) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "evaluate");
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_synchronize(fmmx_ctx* ctx) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "synchronize");
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_get_stats(const fmmx_ctx* ctx, fmmx_stats* out) {
+    if (!ctx || !out) return FMMX_INVALID_ARG;
+    *out = ctx->st;
+    out->n = ctx->n;
+    out->n_cells = ctx->nc;
+    out->n_leaves = ctx->nleaves;
+    out->n_levels = ctx->nlevels;
+    out->n_m2l = ctx->n_m2l;
+    out->n_p2p = ctx->n_p2p;
+    out->walk_pops = ctx->pops;
+    out->p2p_interactions = ctx->p2p_inter;
+    out->m2l_directed = 2ull * (uint64_t)ctx->n_m2l;
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_export_tree(const fmmx_ctx* cctx, uint32_t* order, uint64_t* keys_sorted, uint32_t* cell_info,
+                             int32_t* children, double* cen, double* mass, double* rho) {
+    fmmx_ctx* ctx = const_cast<fmmx_ctx*>(cctx);
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "export before build");
+    cudaSetDevice(ctx->cfg.device);
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    const size_t n = ctx->n, nc = ctx->nc;
+    if (order) CK(cudaMemcpy(order, ctx->order.p, n * 4, cudaMemcpyDeviceToHost), "copy");
+    if (keys_sorted) CK(cudaMemcpy(keys_sorted, ctx->keys_sorted.p, n * 8, cudaMemcpyDeviceToHost), "copy");
+    if (cell_info) {
+        std::vector<uint32_t> f(nc), c(nc);
+        std::vector<uint8_t> lv(nc), lf(nc);
+        CK(cudaMemcpy(f.data(), ctx->c_first.p, nc * 4, cudaMemcpyDeviceToHost), "copy");
+        CK(cudaMemcpy(c.data(), ctx->c_count.p, nc * 4, cudaMemcpyDeviceToHost), "copy");
+        CK(cudaMemcpy(lv.data(), ctx->c_level.p, nc, cudaMemcpyDeviceToHost), "copy");
+        CK(cudaMemcpy(lf.data(), ctx->c_leaf.p, nc, cudaMemcpyDeviceToHost), "copy");
+        for (size_t i = 0; i < nc; ++i) {
+            cell_info[4 * i] = f[i];
+            cell_info[4 * i + 1] = c[i];
+            cell_info[4 * i + 2] = lv[i];
+            cell_info[4 * i + 3] = lf[i];
+        }
+    }
+    if (children) CK(cudaMemcpy(children, ctx->c_child.p, nc * 8 * 4, cudaMemcpyDeviceToHost), "copy");
+    if (cen) {
+        std::vector<double> a(nc), b(nc), c(nc);
+        CK(cudaMemcpy(a.data(), ctx->c_cx.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+        CK(cudaMemcpy(b.data(), ctx->c_cy.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+        CK(cudaMemcpy(c.data(), ctx->c_cz.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+        for (size_t i = 0; i < nc; ++i) {
+            cen[3 * i] = a[i];
+            cen[3 * i + 1] = b[i];
+            cen[3 * i + 2] = c[i];
+        }
+    }
+    if (mass) CK(cudaMemcpy(mass, ctx->c_mass.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+    if (rho) CK(cudaMemcpy(rho, ctx->c_rho.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_export_lists(const fmmx_ctx* cctx, uint32_t* m2l, uint32_t* p2p) {
+    fmmx_ctx* ctx = const_cast<fmmx_ctx*>(cctx);
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!ctx->evaluated) return fail(ctx, FMMX_NOT_BUILT, "export before evaluate");
+    cudaSetDevice(ctx->cfg.device);
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    if (m2l && ctx->n_m2l) CK(cudaMemcpy(m2l, ctx->m2l.p, (size_t)ctx->n_m2l * 8, cudaMemcpyDeviceToHost), "copy");
+    if (p2p && ctx->n_p2p) CK(cudaMemcpy(p2p, ctx->p2p.p, (size_t)ctx->n_p2p * 8, cudaMemcpyDeviceToHost), "copy");
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_export_expansions(const fmmx_ctx* cctx, double* moments, double* locals, double* pows, double* f,
+                                   double* fmin) {
+    fmmx_ctx* ctx = const_cast<fmmx_ctx*>(cctx);
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!ctx->evaluated) return fail(ctx, FMMX_NOT_BUILT, "export before evaluate");
+    cudaSetDevice(ctx->cfg.device);
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    const size_t nc = ctx->nc, dim = dimp(ctx->cfg.p);
+    if (moments) CK(cudaMemcpy(moments, ctx->moments.p, nc * dim * 16, cudaMemcpyDeviceToHost), "copy");
+    if (locals) CK(cudaMemcpy(locals, ctx->locals.p, nc * dim * 16, cudaMemcpyDeviceToHost), "copy");
+    if (pows) CK(cudaMemcpy(pows, ctx->pows.p, nc * (ctx->cfg.p + 1) * 8, cudaMemcpyDeviceToHost), "copy");
+    if (f && ctx->cfg.mac_mode == FMMX_MAC_DEHNEN) CK(cudaMemcpy(f, ctx->f.p, ctx->n * 8, cudaMemcpyDeviceToHost), "copy");
+    if (fmin && ctx->cfg.mac_mode == FMMX_MAC_DEHNEN)
+        CK(cudaMemcpy(fmin, ctx->fmin.p, nc * 8, cudaMemcpyDeviceToHost), "copy");
+    return FMMX_OK;
+}
+
+fmmx_status fmmx_direct_targets(int device, size_t n, const double* pos, const double* mass, double softening,
+                                size_t nt, const uint32_t* targets, double* acc, double* pot, double* fscale) {
+    if (!pos || !mass || !targets || !acc || n == 0) return FMMX_INVALID_ARG;
+    if (nt == 0) return FMMX_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FMMX_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return FMMX_INVALID_ARG;
+    for (size_t q = 0; q < nt; ++q)
+        if (targets[q] >= n) return FMMX_INVALID_ARG;
+    cudaSetDevice(device);
+    const int nsplit = 32;
+    double *dpos = nullptr, *dmass = nullptr, *part = nullptr, *dacc = nullptr, *dpot = nullptr, *df = nullptr;
+    uint32_t* dt = nullptr;
+    fmmx_status st = FMMX_OK;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&dpos, 3 * n * 8) != cudaSuccess || cudaMalloc(&dmass, n * 8) != cudaSuccess ||
+        cudaMalloc(&dt, nt * 4) != cudaSuccess || cudaMalloc(&part, nsplit * nt * 5 * 8) != cudaSuccess ||
+        cudaMalloc(&dacc, nt * 3 * 8) != cudaSuccess || cudaMalloc(&dpot, nt * 8) != cudaSuccess ||
+        cudaMalloc(&df, nt * 8) != cudaSuccess) {
+        st = FMMX_OUT_OF_MEMORY;
+    } else {
+        cudaMemcpyAsync(dpos, pos, 3 * n * 8, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dmass, mass, n * 8, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dt, targets, nt * 4, cudaMemcpyHostToDevice, s);
+        dim3 g((unsigned)((nt + 127) / 128), nsplit);
+        k_direct_targets<<<g, 128, 0, s>>>(dpos, dmass, n, dt, nt, softening * softening, part);
+        k_direct_reduce<<<grid_for(nt, 128), 128, 0, s>>>(part, nsplit, nt, dacc, dpot, df);
+        cudaMemcpyAsync(acc, dacc, nt * 3 * 8, cudaMemcpyDeviceToHost, s);
+        if (pot) cudaMemcpyAsync(pot, dpot, nt * 8, cudaMemcpyDeviceToHost, s);
+        if (fscale) cudaMemcpyAsync(fscale, df, nt * 8, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) st = FMMX_DEVICE_ERROR;
+    }
+    for (void* q : {(void*)dpos, (void*)dmass, (void*)dt, (void*)part, (void*)dacc, (void*)dpot, (void*)df})
+        if (q) cudaFree(q);
+    if (s) cudaStreamDestroy(s);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// Kernel declarations and the device-side structures shared between the
+// kernel files and the host orchestration (engine.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace fmmx {
+
+// Level bookkeeping array: start and count of each level's nodes.
+enum { LV_START = 0, LV_COUNT = FMMX_NLEVELS + 1, LV_SIZE = 2 * (FMMX_NLEVELS + 1) };
+
+// Nodes as created level by level, before depth-first renumbering.
+struct TmpNodes {
+    uint32_t* first;
+    uint32_t* count;
+    int32_t* parent;
+    uint8_t* oct;
+    uint8_t* level;
+    uint8_t* leaf;
+};
+
+struct CellsMut {
+    uint32_t* first;
+    uint32_t* count;
+    int32_t* child;
+    int32_t* parent;
+    uint8_t* leaf;
+    uint8_t* level;
+    double* cx;
+    double* cy;
+    double* cz;
+    double* mass;
+    double* rho;
+};
+
+struct MacParams {
+    int mode;  // fmmx_mac_mode
+    int p;
+    double eps;
+    double theta;
+};
+
+enum { WC_FRONT0 = 0, WC_FRONT1 = 1, WC_M2L = 2, WC_P2P = 3, WC_OVERFLOW = 4, WC_SIZE = 8 };
+
+struct WalkBufs {
+    uint2* front[2];
+    uint2* m2l;
+    uint2* p2p;
+    int* counts;           // WC_* slots
+    unsigned long long* pops_ptr;
+    uint32_t cap_front, cap_m2l, cap_p2p;
+};
+
+// Segmented directed interaction list: for destination cell c, sources
+// src[seg_begin[c] .. seg_end[c]) (ascending).
+struct DirList {
+    const uint64_t* keys;  // (dst << 32) | src, sorted
+    const uint32_t* seg_begin;
+    const uint32_t* seg_end;
+};
+
+// tree_exact.cu
+void upload_tables_exact(const OrderTables& t, cudaStream_t s);
+__global__ void k_bbox_partial(const double* pos, size_t n, double* part, int* bad);
+__global__ void k_bbox_final(const double* part, int nparts, double* box);
+__global__ void k_keys(const double* pos, size_t n, const double* box, uint64_t* keys, uint32_t* idx);
+__global__ void k_gather(const double* pos, const double* mass, const uint32_t* order, size_t n, double* x,
+                         double* y, double* z, double* m);
+__global__ void k_tree_init(TmpNodes t, uint32_t n, int* lvl);
+__global__ void k_build_level(TmpNodes t, const uint64_t* keys, int L, long long n_leaf, uint32_t cap, int* lvl,
+                              int* flags);
+__global__ void k_dfs_keys(TmpNodes t, int nc, uint64_t* key, uint32_t* val);
+__global__ void k_finalize_cells(const uint32_t* sorted_t, int nc, TmpNodes t, int32_t* new_id, CellsMut cells);
+__global__ void k_link_cells(int nc, TmpNodes t, const int32_t* new_id, CellsMut cells, int32_t* level_cells);
+__global__ void k_body_leaf(int nc, const uint32_t* first, const uint32_t* count, const uint8_t* leaf,
+                            int32_t* body_leaf);
+__global__ void k_geometry_level(const int32_t* level_cells, int lstart, int lcnt, CellsMut cells, const double* x,
+                                 const double* y, const double* z, const double* m, int center_mode);
+__global__ void k_upward_exact(const int32_t* level_cells, int lstart, int lcnt, CellsView cells, const double* x,
+                               const double* y, const double* z, const double* m, int p, zd* moments, double* pows,
+                               const double* f, double* fmin);
+__global__ void k_fprepass(CellsView cells, const double* x, const double* y, const double* z, const double* m,
+                           size_t n, double* f, int* err);
+__global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
+
+// lists.cu
+__global__ void k_expand_m2l(const uint2* pairs, int np, uint64_t* keys);
+__global__ void k_expand_p2p(const uint2* pairs, int np, const uint32_t* count, uint64_t sentinel, uint64_t* keys,
+                             unsigned long long* interactions);
+__global__ void k_segments(const uint64_t* keys, int nkeys, uint32_t* seg_begin, uint32_t* seg_end);
+
+// m2l.cu
+void upload_tables_m2l(const OrderTables& t, cudaStream_t s);
+size_t m2l_rot_smem_bytes(int p);
+__global__ void k_m2l_naive_f64(DirList L, int ncells, CellsView cv, int p, const zd* moments, zd* locals);
+__global__ void k_m2l_rot_f64(DirList L, int ncells, CellsView cv, int p, const zd* moments, zd* locals,
+                              const double* swap_g);
+
+// sweeps.cu
+void upload_tables_sweeps(const OrderTables& t, cudaStream_t s);
+__global__ void k_l2l_f64(const int32_t* level_cells, int lstart, int lcnt, CellsView cv, const int32_t* parent,
+                          int p, zd* locals);
+__global__ void k_l2p_f64(size_t n, const int32_t* body_leaf, const uint32_t* order, CellsView cv, int p,
+                          const zd* locals, const double* x, const double* y, const double* z, const double* nax,
+                          const double* nay, const double* naz, const double* npot, double* acc, double* pot);
+
+// p2p.cu
+__global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,
+                          const double* m, double soft2, double* ax, double* ay, double* az, double* pot);
+
+// direct.cu
+__global__ void k_direct_targets(const double* pos, const double* mass, size_t n, const uint32_t* tgt, size_t nt,
+                                 double soft2, double* part);
+__global__ void k_direct_reduce(const double* part, int nsplit, size_t nt, double* acc, double* pot, double* fsc);
+
+}  // namespace fmmx
