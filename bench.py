@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark of the FMM force evaluation on B200.
+
+Metric: bodies/s of one complete force evaluation (tree build, upward pass,
+dual walk, M2L, L2L, P2P, L2P) on one GPU, with the p50/p99 relative force
+error against an FP64 direct sum on 4096 seeded targets beside it.
+
+Workload (default, --config c2): N = 1,048,576 bodies uniform in the unit cube,
+log-normal masses (mu 0, sigma 0.5) normalised to 1, Plummer softening 1e-4,
+p = 10, opening angle 0.5, leaf capacity 64; seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|plain]
+    python bench.py --impl reference ...   # CPU FMM (the oracle's restatement)
+
+Under torchrun every rank runs its own replica (the evaluation does not shard;
+no collective on the data path); rank 0 prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c1": dict(gen="plummer_ic", n=16384, p=8, theta=0.5, softening=1e-3, n_leaf=64,
+               workload="Plummer N=16384 (r<=20, DF velocities), softening 1e-3, p=8, theta=0.5, leaf 64"),
+    "c2": dict(gen="uniform", n=1 << 20, p=10, theta=0.5, softening=1e-4, n_leaf=64,
+               workload="uniform cube N=1048576, log-normal masses sigma=0.5, softening 1e-4, p=10, theta=0.5, leaf 64"),
+    "c3": dict(gen="clusters", n=1 << 22, p=12, theta=0.4, softening=1e-5, n_leaf=32,
+               workload="64 Plummer clusters N=4194304, a log-uniform[1e-3,1e-1], softening 1e-5, p=12, theta=0.4, leaf 32"),
+}
+SEEDS = {"plummer_ic": 11, "uniform": 22, "clusters": 33}
+METRIC = "bodies/s at p99 force err <=1e-5 (mixed vs FP64 plain, 1 B200); p50/p99 step ms"
+
+
+def make_inputs(fx, cfg):
+    n = cfg["n"]
+    if cfg["gen"] == "uniform":
+        mass, pos = fx.gen_uniform_lognormal(n, 0.5, SEEDS["uniform"])
+    elif cfg["gen"] == "plummer_ic":
+        mass, pos, _ = fx.gen_plummer_ic(n, 1.0, 1.0, 20.0, SEEDS["plummer_ic"])
+    else:
+        mass, pos, _ = fx.gen_clusters(n, 64, 1e-3, 1e-1, SEEDS["clusters"])
+    return mass, pos
+
+
+# ------------------------------------------------------------------ roofline
+def m2l_flops_per_translation(p: int, kernel: str) -> float:
+    """Flops (FMA = 2) of one directed M2L translation as the kernel runs it.
+
+    rotation (warp kernel, m >= 0 half basis): per degree of K = k+1 terms the
+    back rotation costs 8K^2 + 13K and the forward 8K^2 + 12K; the axial
+    translation 4 per (n, m, k) term plus 4 per output; the lane reduction 2
+    per output; phases and geometry about 12(p+1) + 50.
+    naive: 8 per complex term of sum_{n,m} (p-n+1)^2 (translate.rs:47-136).
+    """
+    if kernel == "naive":
+        return 8.0 * sum((2 * n + 1) * (p - n + 1) ** 2 for n in range(p + 1))
+    h = (p + 1) * (p + 2) // 2
+    rot = sum(16 * K * K + 25 * K for K in range(1, p + 2))
+    axial = sum(max(0, p - n - m + 1) for m in range(p + 1) for n in range(m, p + 1))
+    return rot + 4 * axial + 6 * h + 12 * (p + 1) + 50
+
+
+def p2p_flops(interactions: int) -> float:
+    """16 flops per directed body-body interaction (crates/fmm/src/roofline.rs:15-19)."""
+    return 16.0 * interactions
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_fmm_sample(cfg, sample_n, nthreads, fx):
+    """Time the oracle's restatement of the reference FMM (threaded run_impl)
+    on a bounded sample of the workload; returns (bodies/s, seconds)."""
+    import oracle
+
+    sub = dict(cfg)
+    sub["n"] = sample_n
+    mass, pos = make_inputs(fx, sub)
+    t0 = time.perf_counter()
+    f = oracle.Fmm(mass, pos, cfg["p"], 0.0, cfg["n_leaf"], mac=oracle.MAC_THETA, theta=cfg["theta"],
+                   softening=cfg["softening"])
+    f.run(nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return sample_n / dt, dt
+
+
+def run_reference(args, cfg, rank):
+    """--impl reference: the reference's CPU FMM (restated in oracle/, the
+    Rust reference cannot be built here) on the box's host cores."""
+    if rank != 0:
+        return
+    import fmms_b200 as fx
+
+    nthreads = os.cpu_count() or 1
+    sample_n = args.cpu_sample
+    times = []
+    for i in range(args.warmup + args.steps):
+        bps, dt = cpu_fmm_sample(cfg, sample_n, nthreads, fx)
+        if i >= args.warmup:
+            times.append(dt)
+    mean = sum(times) / len(times)
+    value = sample_n / mean
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "sample_bodies": sample_n},
+        "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{sample_n} bodies of the same generator and settings, one threaded "
+                                   f"evaluation per step (oracle/fmm_oracle.cpp run_impl)"},
+        "e2e": {"value": value, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_gpu(args, cfg, rank, world, local_rank):
+    import torch
+
+    import fmms_b200 as fx
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    mass, pos = make_inputs(fx, cfg)
+    n = len(mass)
+    d_pos = torch.from_numpy(pos).to(f"cuda:{dev}")
+    d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+    d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    kw = dict(mac="theta", theta=cfg["theta"], softening=cfg["softening"], precision=args.precision, m2l=args.m2l,
+              device=dev, stream=stream.cuda_stream)
+    g = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], **kw)
+
+    def step():
+        g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+        g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    times, m2l_ms, p2p_ms, st = [], [], [], None
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (untimed)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            st = g.stats()
+            m2l_ms.append(st["ms_m2l"])
+            p2p_ms.append(st["ms_p2p"])
+    torch.cuda.synchronize()
+    total_ms = sum(times)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    # end to end through the host API: pinned host inputs in, host results out
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_acc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    h_pot = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st_b = fx.lib().fmmx_build(g._h, n, fx._ptr(h_pos.numpy()), fx._ptr(h_mass.numpy()))
+        st_e = fx.lib().fmmx_evaluate(g._h, None, None, fx._ptr(h_acc.numpy()), fx._ptr(h_pot.numpy()))
+        e1.record(stream)
+        e1.synchronize()
+        assert st_b == 0 and st_e == 0, fx.lib().fmmx_last_error(g._h)
+        if i >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+
+    # accuracy against the FP64 direct sum on 4096 seeded targets
+    rng = np.random.default_rng(4096)
+    tg = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.uint32)
+    a_ref, _, _ = fx.direct_targets(mass, pos, tg, softening=cfg["softening"], device=dev)
+    acc = h_acc.numpy()
+    rel = np.linalg.norm(acc[tg] - a_ref, axis=1) / np.linalg.norm(a_ref, axis=1)
+
+    if rank != 0:
+        return
+    # roofline of the dominant kernel (M2L), from its own CUDA events
+    kernel = "naive" if args.m2l == "naive" else "rotation"
+    fl = st["m2l_directed"] * m2l_flops_per_translation(cfg["p"], kernel)
+    m2l_avg = sum(m2l_ms) / len(m2l_ms)
+    fp64 = args.precision == "plain"
+    peak = fx.probe_fma_peak(fp64=fp64, device=dev)
+    achieved = fl / (m2l_avg * 1e-3) / 1e12
+    roof = {"bound": "fp64" if fp64 else "fp32", "kernel": "m2l", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "peak_source": "measured: FMA loop on every SM (fmmx_probe_fma_peak); MEASURED_PEAKS.json holds only "
+                           "HBM and bf16-tensor peaks",
+            "algorithmic_flops_per_launch": fl, "launch_ms": m2l_avg,
+            "p2p": {"achieved": p2p_flops(st["p2p_interactions"]) / (sum(p2p_ms) / len(p2p_ms) * 1e-3) / 1e12,
+                    "unit": "TFLOP/s", "ms": sum(p2p_ms) / len(p2p_ms)}}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nth = os.cpu_count() or 1
+        bps, dt = cpu_fmm_sample(cfg, args.cpu_sample, nth, fx)
+        cpu = {"value": bps, "unit": "bodies/s", "cores": nth, "kind": "port",
+               "sample": f"{args.cpu_sample} bodies of the same generator and settings, one threaded evaluation "
+                         f"of the oracle's restatement of the reference FMM ({dt:.1f} s)"}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "precision": args.precision, "n": n, "p": cfg["p"],
+                   "theta": cfg["theta"], "n_leaf": cfg["n_leaf"], "l2": "flushed between timed steps",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "step_ms_p50": float(np.percentile(times, 50)), "step_ms_p99": float(np.percentile(times, 99)),
+        "force_err": {"p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99)),
+                      "max": float(rel.max()), "targets": len(tg), "reference": "FP64 direct sum"},
+        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "bodies/s", "h2d_bytes_per_step": 32 * n,
+                "d2h_bytes_per_step": 32 * n, "ms_per_step": e2e_ms},
+        "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "stages_ms": {k[3:]: round(v, 3) for k, v in st.items() if k.startswith("ms_")},
+        "counts": {k: int(st[k]) for k in ("n_cells", "n_leaves", "n_m2l", "n_p2p", "p2p_interactions")},
+        "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    g.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fmmx", choices=["fmmx", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
+    ap.add_argument("--cpu-sample", type=int, default=262144)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_gpu(args, cfg, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

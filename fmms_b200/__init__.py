@@ -88,6 +88,7 @@ class Stats(C.Structure):
         ("ms_l2l", C.c_double),
         ("ms_l2p", C.c_double),
         ("ms_evaluate", C.c_double),
+        ("kernel_launches", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -119,8 +120,12 @@ SIGNATURES = {
     "fmmx_export_lists": (_st, [_vp, _u32p, _u32p]),
     "fmmx_export_expansions": (_st, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "fmmx_direct_targets": (_st, [C.c_int, _sz, _dp, _dp, C.c_double, _sz, _u32p, _dp, _dp, _dp]),
+    "fmmx_probe_fma_peak": (_st, [C.c_int, C.c_int, _dp]),
     "fmmx_gen_plummer": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]),
     "fmmx_gen_hernquist": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]),
+    "fmmx_gen_plummer_ic": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp, _dp]),
+    "fmmx_gen_uniform_lognormal": (None, [_sz, C.c_double, C.c_uint64, _dp, _dp]),
+    "fmmx_gen_clusters": (None, [_sz, C.c_int, C.c_double, C.c_double, C.c_uint64, _dp, _dp, _dp]),
 }
 
 
@@ -337,3 +342,38 @@ def gen_hernquist(n, center=(0.0, 0.0, 0.0), seed=7):
     pos = np.empty((n, 3))
     lib().fmmx_gen_hernquist(n, center[0], center[1], center[2], seed, _ptr(mass), _ptr(pos))
     return mass, pos
+
+
+def gen_plummer_ic(n, mtot=1.0, a=1.0, rmax=20.0, seed=1, velocities=True):
+    """Truncated Plummer sphere with Plummer-DF velocities -> (mass, pos, vel)."""
+    mass = np.empty(n)
+    pos = np.empty((n, 3))
+    vel = np.empty((n, 3)) if velocities else None
+    lib().fmmx_gen_plummer_ic(n, mtot, a, rmax, seed, _ptr(mass), _ptr(pos), _ptr(vel))
+    return mass, pos, vel
+
+
+def gen_uniform_lognormal(n, sigma=0.5, seed=2):
+    """Uniform unit cube, log-normal masses normalised to 1 -> (mass, pos)."""
+    mass = np.empty(n)
+    pos = np.empty((n, 3))
+    lib().fmmx_gen_uniform_lognormal(n, sigma, seed, _ptr(mass), _ptr(pos))
+    return mass, pos
+
+
+def gen_clusters(n, nclust=64, amin=1e-3, amax=1e-1, seed=3, velocities=True):
+    """nclust Plummer spheres (Dirichlet(1) sizes) -> (mass, pos, vel)."""
+    mass = np.empty(n)
+    pos = np.empty((n, 3))
+    vel = np.empty((n, 3)) if velocities else None
+    lib().fmmx_gen_clusters(n, nclust, amin, amax, seed, _ptr(mass), _ptr(pos), _ptr(vel))
+    return mass, pos, vel
+
+
+def probe_fma_peak(fp64: bool, device: int = 0) -> float:
+    """Measured FMA throughput (TFLOP/s) of the device, FP64 or FP32."""
+    out = C.c_double()
+    st = lib().fmmx_probe_fma_peak(device, int(fp64), C.byref(out))
+    if st != 0:
+        raise FmmError(st, "fmmx_probe_fma_peak failed")
+    return out.value

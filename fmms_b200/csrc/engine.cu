@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "rotw.h"
 #include "sort.h"
 
 using namespace fmmx;
@@ -50,6 +51,8 @@ struct DBuf {
         return cudaSuccess;
     }
 };
+
+int rot_moff_host(int k) { return 4 * (k * (k + 1) * (2 * k + 1) / 6); }
 
 int bits_for(uint64_t v) {
     int b = 0;
@@ -113,6 +116,10 @@ struct fmmx_ctx {
     // expansions
     DBuf<zd> moments, locals;
     DBuf<double> pows, f, fmin;
+    // mixed form: normalised FP32 half-layout expansions and the per-cell length
+    DBuf<zf> mom_f, loc_f;
+    DBuf<double> ell;
+    DBuf<float> ellf;
 
     // walk
     DBuf<uint2> front0, front1, m2l, p2p;
@@ -123,6 +130,10 @@ struct fmmx_ctx {
     // directed lists
     DBuf<uint64_t> m2l_keys, m2l_keys_s, p2p_keys, p2p_keys_s;
     DBuf<uint32_t> m2l_seg_b, m2l_seg_e, p2p_seg_b, p2p_seg_e;
+
+    DBuf<int> work;  // persistent-kernel work counter
+    int nsm = 148;
+    uint64_t launches = 0, launches_build = 0;
 
     fmmx_stats st;
     cudaEvent_t ev[12];
@@ -150,6 +161,8 @@ fmmx_status cuda_fail(fmmx_ctx* c, cudaError_t e, const char* where) {
     } while (0)
 
 #define CKL(where) CK(cudaGetLastError(), where)
+// kernel launches of the current build/evaluate (reported in fmmx_stats)
+#define LCOUNT(k) (ctx->launches += (k))
 
 CellsView view(fmmx_ctx* c) {
     CellsView v;
@@ -214,6 +227,54 @@ void build_swap(int p, std::vector<double>& sw) {
     }
 }
 
+}  // namespace
+
+// Real half-basis forms of the swap matrices for the warp rotation M2L.
+void fmmx::make_rotw_tables(RotwTables& t) {
+    const int P = kRotwMaxP;
+    std::vector<double> sw;
+    build_swap(P, sw);
+    auto boff = [](int j) { return j == 0 ? 0 : j * (4 * j * j - 1) / 3; };
+    t.mats.assign(rot_moff_host(P + 1), 0.0);
+    for (int k = 0; k <= P; ++k) {
+        const int nb = 2 * k + 1, off = boff(k), kk = (k + 1) * (k + 1);
+        auto B = [&](int r, int c) { return sw[off + (r + k) * nb + (c + k)]; };
+        double* Pm = t.mats.data() + rot_moff_host(k);
+        double* Qm = Pm + kk;
+        double* PT = Qm + kk;
+        double* QT = PT + kk;
+        for (int r = 0; r <= k; ++r)
+            for (int c = 0; c <= k; ++c) {
+                const double sg = (c & 1) ? -1.0 : 1.0;
+                if (c == 0) {
+                    Pm[r * (k + 1)] = B(r, 0);
+                    Qm[r * (k + 1)] = B(r, 0);
+                    PT[r * (k + 1)] = B(0, r);
+                    QT[r * (k + 1)] = B(0, r);
+                } else {
+                    Pm[r * (k + 1) + c] = B(r, c) + sg * B(r, -c);
+                    Qm[r * (k + 1) + c] = B(r, c) - sg * B(r, -c);
+                    PT[r * (k + 1) + c] = B(c, r) + sg * B(-c, r);
+                    QT[r * (k + 1) + c] = B(c, r) - sg * B(-c, r);
+                }
+            }
+    }
+    std::vector<double> f(2 * P + 1, 1.0);
+    for (int i = 1; i <= 2 * P; ++i) f[i] = f[i - 1] * (double)i;
+    t.fact = f;
+    const int nh = P * (P + 1) / 2 + P + 1;
+    t.fm.assign(nh, 0.0);
+    t.ifm.assign(nh, 0.0);
+    for (int n = 0; n <= P; ++n)
+        for (int m = 0; m <= n; ++m) {
+            const int h = n * (n + 1) / 2 + m;
+            t.fm[h] = f[n - m] * f[n + m];
+            t.ifm[h] = 1.0 / t.fm[h];
+        }
+}
+
+namespace {
+
 void make_tables(int p, OrderTables& t) {
     std::memset(&t, 0, sizeof(t));
     t.fact[0] = 1.0;
@@ -224,10 +285,14 @@ void make_tables(int p, OrderTables& t) {
         for (int m = 0; m < n; ++m) t.invc[n][m] = 1.0 / (double)(n * n - m * m);
 }
 
-bool use_rotation(const fmmx_config& c) {
-    if (c.m2l_kernel == FMMX_M2L_ROTATION) return true;
-    if (c.m2l_kernel == FMMX_M2L_NAIVE) return false;
-    return c.p >= 20;  // rotation.rs:45 ROT_P
+enum M2lChoice { M2L_NAIVE_BLOCK, M2L_ROT_BLOCK, M2L_ROT_WARP };
+
+// AUTO and ROTATION take the warp rotation kernel where its constant tables
+// reach (p <= 16), else the block rotation kernel; NAIVE keeps the reference's
+// O(p^4) convolution.
+M2lChoice m2l_choice(const fmmx_config& c) {
+    if (c.m2l_kernel == FMMX_M2L_NAIVE) return M2L_NAIVE_BLOCK;
+    return c.p <= kRotwMaxP ? M2L_ROT_WARP : M2L_ROT_BLOCK;
 }
 
 const unsigned kGrid = 148u * 8u;
@@ -253,7 +318,9 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
     CK(ctx->flags.ensure(8), "alloc flags");
     CK(cudaMemsetAsync(ctx->flags.p, 0, 8 * sizeof(int), s), "memset");
 
+    ctx->launches = 0;
     k_bbox_partial<<<gb, 256, 0, s>>>(d_pos, n, ctx->bbox_part.p, ctx->flags.p + 2);
+    LCOUNT(5);  // bbox (2), keys, key sort (onesweep passes counted as 1), gather
     k_bbox_final<<<1, 32, 0, s>>>(ctx->bbox_part.p, (int)gb, ctx->box.p);
     k_keys<<<grid_for(n, 256), 256, 0, s>>>(d_pos, n, ctx->box.p, ctx->keys.p, ctx->idx.p);
     CKL("keys");
@@ -286,6 +353,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
         CK(cudaMemsetAsync(ctx->lvl.p, 0, LV_SIZE * sizeof(int), s), "memset");
         CK(cudaMemsetAsync(ctx->flags.p, 0, 2 * sizeof(int), s), "memset");
         k_tree_init<<<1, 32, 0, s>>>(tn, (uint32_t)n, ctx->lvl.p);
+        LCOUNT(1 + FMMX_NLEVELS);
         const unsigned gl = std::min<unsigned>(grid_for(cap, 256), kGrid);
         for (int L = 0; L < FMMX_NLEVELS; ++L)
             k_build_level<<<gl, 256, 0, s>>>(tn, ctx->keys_sorted.p, L, (long long)ctx->cfg.n_leaf, cap, ctx->lvl.p,
@@ -321,6 +389,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
     CK(ctx->dfs_val_alt.ensure(nc), "alloc");
     CK(ctx->new_id.ensure(nc), "alloc");
     k_dfs_keys<<<grid_for(nc, 256), 256, 0, s>>>(tn, nc, ctx->dfs_key.p, ctx->dfs_val.p);
+    LCOUNT(5 + nlev);  // dfs keys, sort, finalize, link, body->leaf, geometry per level
     const int dbits = 5 + bits_for(n);
     tb = sort_pairs_u64_u32_temp(nc, dbits);
     CK(ctx->cub_tmp.ensure(tb), "alloc sort");
@@ -358,6 +427,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
     }
     ctx->build_pos = d_pos;
     ctx->build_mass = d_mass;
+    ctx->launches_build = ctx->launches;
     ctx->built = true;
     return FMMX_OK;
 }
@@ -406,6 +476,7 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
         for (int it = 0; it < max_iter && !done;) {
             for (int b = 0; b < 6; ++b, ++it) {
                 k_walk_iter<<<kGrid, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
+                LCOUNT(1);
                 CK(cudaMemsetAsync(ctx->wcounts.p + cur, 0, sizeof(int), s), "memset");
                 cur ^= 1;
             }
@@ -447,6 +518,7 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
         CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
         CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
         k_expand_m2l<<<grid_for(nm, 256), 256, 0, s>>>(ctx->m2l.p, nm, ctx->m2l_keys.p);
+        LCOUNT(3);
         size_t tb = sort_keys_u64_temp(2 * nm, cbits);
         CK(ctx->cub_tmp.ensure(tb), "alloc sort");
         CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
@@ -466,6 +538,7 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
         CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
         CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
         const uint64_t sentinel = (uint64_t)nc << 32;
+        LCOUNT(3);
         k_expand_p2p<<<grid_for(np, 256), 256, 0, s>>>(ctx->p2p.p, np, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
                                                        ctx->inter.p);
         size_t tb = sort_keys_u64_temp(2 * np, cbits);
@@ -479,6 +552,46 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     return FMMX_OK;
 }
 
+// Mixed form: FP32 M2L/L2L/L2P on normalised expansions, FP32 + double-single
+// P2P; events 5..9 as in the plain path.
+fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirList& lp, double* d_acc,
+                                    double* d_pot) {
+    cudaStream_t s = ctx->stream;
+    const int p = ctx->cfg.p, nc = ctx->nc, H = (p + 1) * (p + 2) / 2;
+    const size_t n = ctx->n;
+    const CellsView cv = view(ctx);
+    cudaEvent_t* ev = ctx->ev;
+    const bool tm = ctx->events;
+    CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * H * sizeof(zf), s), "memset");
+    if (ctx->n_m2l > 0) {
+        if (p > kRotwMaxP) return fail(ctx, FMMX_INVALID_ARG, "mixed precision supports p <= 16");
+        CK(ctx->work.ensure(1), "alloc");
+        CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
+        CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, ctx->work.p, ctx->nsm, s), "m2l");
+    }
+    if (tm) CK(cudaEventRecord(ev[6], s), "event");
+    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 2);
+    for (int L = 1; L < ctx->nlevels; ++L) {
+        const int cnt = ctx->lvl_count[L];
+        const unsigned g = std::min<unsigned>(cnt, 148u * 16u);
+        launch_l2l_mixed(L <= 3, g, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->c_parent.p, ctx->ell.p,
+                         p, ctx->loc_f.p);
+    }
+    CKL("l2l (mixed)");
+    if (tm) CK(cudaEventRecord(ev[7], s), "event");
+    const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
+    k_p2p_mixed<<<std::min<unsigned>(nc, 148u * 16u), 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
+                                                                    ctx->m.p, soft2, ctx->nax.p, ctx->nay.p,
+                                                                    ctx->naz.p, ctx->npot.p);
+    CKL("p2p (mixed)");
+    if (tm) CK(cudaEventRecord(ev[8], s), "event");
+    k_l2p_mixed<<<grid_for(n, 128), 128, 0, s>>>(n, ctx->body_leaf.p, ctx->order.p, cv, ctx->ell.p, p,
+                                                 ctx->loc_f.p, ctx->x.p, ctx->y.p, ctx->z.p, ctx->nax.p,
+                                                 ctx->nay.p, ctx->naz.p, ctx->npot.p, d_acc, d_pot);
+    CKL("l2p (mixed)");
+    return FMMX_OK;
+}
+
 fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
     cudaStream_t s = ctx->stream;
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
@@ -487,24 +600,47 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     cudaEvent_t* ev = ctx->ev;
     const bool tm = ctx->events;
     if (tm) CK(cudaEventRecord(ev[2], s), "event");
+    ctx->launches = ctx->launches_build;
     if (d_pos == nullptr) d_pos = ctx->build_pos;
     if (d_mass == nullptr) d_mass = ctx->build_mass;
     k_gather<<<grid_for(n, 256), 256, 0, s>>>(d_pos, d_mass, ctx->order.p, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p);
     CKL("gather");
+    LCOUNT(1 + ctx->nlevels + (ctx->cfg.mac_mode == FMMX_MAC_DEHNEN ? 1 : 0));  // gather, upward levels, f pre-pass
     CK(ctx->moments.ensure((size_t)nc * dim), "alloc expansions");
     CK(ctx->locals.ensure((size_t)nc * dim), "alloc expansions");
     CK(ctx->pows.ensure((size_t)nc * (p + 1)), "alloc expansions");
     CK(ctx->fmin.ensure(nc), "alloc expansions");
     CK(ctx->f.ensure(n), "alloc expansions");
     const bool dehnen = ctx->cfg.mac_mode == FMMX_MAC_DEHNEN;
+    const bool mixed = ctx->cfg.precision == FMMX_MIXED;
+    const int H = (p + 1) * (p + 2) / 2;
     const CellsView cv = view(ctx);
+    if (mixed) {
+        CK(ctx->mom_f.ensure((size_t)nc * H), "alloc expansions");
+        CK(ctx->loc_f.ensure((size_t)nc * H), "alloc expansions");
+        CK(ctx->ell.ensure(nc), "alloc expansions");
+        CK(ctx->ellf.ensure(nc), "alloc expansions");
+        k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_level.p, ctx->box.p, ctx->ell.p,
+                                                       ctx->ellf.p);
+        LCOUNT(1);
+    }
     if (dehnen) {
         CK(cudaMemsetAsync(ctx->flags.p + 3, 0, sizeof(int), s), "memset");
         k_fprepass<<<grid_for(n, 128), 128, 0, s>>>(cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, n, ctx->f.p,
                                                     ctx->flags.p + 3);
         CKL("f pre-pass");
     }
-    {
+    if (mixed && !dehnen) {
+        // normalised FP32 upward pass; FP64 accumulation on the top three levels
+        const int warps = 4;
+        for (int L = ctx->nlevels - 1; L >= 0; --L) {
+            const int cnt = ctx->lvl_count[L];
+            const unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, kGrid);
+            launch_upward_mixed(L <= 2, g, warps, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->ell.p,
+                                ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->mom_f.p);
+        }
+        CKL("upward (mixed)");
+    } else {
         const int warps = 4;
         const size_t smem = (size_t)warps * 2 * dim * sizeof(zd);
         if (smem > 48 * 1024)
@@ -517,6 +653,12 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
                                                        dehnen ? ctx->f.p : nullptr, ctx->fmin.p);
         }
         CKL("upward");
+        if (mixed) {  // the MAC saw exact FP64 moments; the translations use FP32
+            k_moments_to_mixed<<<grid_for((size_t)nc * H, 256), 256, 0, s>>>(nc, p, ctx->moments.p, ctx->ell.p,
+                                                                            ctx->mom_f.p);
+            LCOUNT(1);
+            CKL("moments to mixed");
+        }
     }
     if (tm) CK(cudaEventRecord(ev[3], s), "event");
     fmmx_status st = walk_impl(ctx);
@@ -533,10 +675,19 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
 
     DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p};
     DirList lp{ctx->p2p_keys_s.p, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p};
+    if (mixed) {
+        fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot);
+        if (ms != FMMX_OK) return ms;
+    } else {
     CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
     if (ctx->n_m2l > 0) {
         const unsigned g = std::min<unsigned>(nc, 148u * 16u);
-        if (use_rotation(ctx->cfg)) {
+        const M2lChoice ch = m2l_choice(ctx->cfg);
+        if (ch == M2L_ROT_WARP) {
+            CK(ctx->work.ensure(1), "alloc");
+            CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
+            CK(launch_rotw_f64(p, lm, nc, cv, ctx->moments.p, ctx->locals.p, ctx->work.p, ctx->nsm, s), "m2l");
+        } else if (ch == M2L_ROT_BLOCK) {
             const size_t smem = m2l_rot_smem_bytes(p);
             CK(cudaFuncSetAttribute(k_m2l_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
             k_m2l_rot_f64<<<g, 128, smem, s>>>(lm, nc, cv, p, ctx->moments.p, ctx->locals.p, ctx->swap_dev.p);
@@ -547,6 +698,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CKL("m2l");
     }
     if (tm) CK(cudaEventRecord(ev[6], s), "event");
+    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 2);  // m2l, l2l per level, p2p, l2p
     {
         const size_t smem = 2 * (size_t)dim * sizeof(zd);
         for (int L = 1; L < ctx->nlevels; ++L) {
@@ -570,6 +722,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
                                                ctx->y.p, ctx->z.p, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p,
                                                d_acc, d_pot);
     CKL("l2p");
+    }
     if (tm) CK(cudaEventRecord(ev[9], s), "event");
     CK(cudaStreamSynchronize(s), "evaluate");
     CK(cudaMemcpy(&ctx->p2p_inter, ctx->inter.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "copy");
@@ -661,10 +814,18 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     }
     ctx->events = true;
     for (int i = 0; i < 12; ++i) cudaEventCreate(&ctx->ev[i]);
+    cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
     make_tables(c.p, ctx->tab);
+    {
+        RotwTables rt;
+        make_rotw_tables(rt);
+        rotw_upload_f64(rt, ctx->stream);
+        rotw_upload_f32(rt, ctx->stream);
+    }
     upload_tables_exact(ctx->tab, ctx->stream);
     upload_tables_m2l(ctx->tab, ctx->stream);
     upload_tables_sweeps(ctx->tab, ctx->stream);
+    upload_tables_mixed(ctx->tab, ctx->stream);
     build_swap(c.p, ctx->swap_host);
     if (ctx->swap_dev.ensure(ctx->swap_host.size()) != cudaSuccess ||
         cudaMemcpyAsync(ctx->swap_dev.p, ctx->swap_host.data(), ctx->swap_host.size() * sizeof(double),
@@ -777,6 +938,7 @@ fmmx_status fmmx_get_stats(const fmmx_ctx* ctx, fmmx_stats* out) {
     out->walk_pops = ctx->pops;
     out->p2p_interactions = ctx->p2p_inter;
     out->m2l_directed = 2ull * (uint64_t)ctx->n_m2l;
+    out->kernel_launches = ctx->launches;
     return FMMX_OK;
 }
 

@@ -104,6 +104,23 @@ __global__ void k_l2p_f64(size_t n, const int32_t* body_leaf, const uint32_t* or
                           const zd* locals, const double* x, const double* y, const double* z, const double* nax,
                           const double* nay, const double* naz, const double* npot, double* acc, double* pot);
 
+// mixed.cu
+void upload_tables_mixed(const OrderTables& t, cudaStream_t s);
+__global__ void k_cell_scale(int nc, const double* rho, const uint8_t* level, const double* box, double* ell,
+                             float* ellf);
+__global__ void k_moments_to_mixed(int nc, int p, const zd* full, const double* ell, zf* half);
+void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
+                         int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,
+                         const double* z, const double* m, int p, zf* mom);
+void launch_l2l_mixed(bool fp64, unsigned grid, cudaStream_t s, const int32_t* level_cells, int lstart, int lcnt,
+                      CellsView cv, const int32_t* parent, const double* ell, int p, zf* loc);
+__global__ void k_l2p_mixed(size_t n, const int32_t* body_leaf, const uint32_t* order, CellsView cv,
+                            const double* ell, int p, const zf* loc, const double* x, const double* y,
+                            const double* z, const double* nax, const double* nay, const double* naz,
+                            const double* npot, double* acc, double* pot);
+__global__ void k_p2p_mixed(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,
+                            const double* m, float soft2, double* ax, double* ay, double* az, double* pot);
+
 // p2p.cu
 __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,
                           const double* m, double soft2, double* ax, double* ay, double* az, double* pot);

@@ -1,0 +1,378 @@
+// Rotation M2L, one lane per directed translation, templated on the
+// arithmetic type T (double for the plain form, float for the mixed form) and
+// the expansion order P.
+//
+// Algorithm (the reference's RotCtx::m2l_pair/apply, rotation.rs:262-435,
+// Dehnen 2014 A.6.1): back-rotate the source multipole with two x<->z swaps
+// B_k around a z-rotation by -β, translate along z with the diagonal kernel
+// F~_n^m = sum_k b_k^{-m} (n+k)!/R^{n+k+1}, rotate forward with B_n^T, and add
+// into the destination's local expansion.
+//
+// B200 structure:
+//  - A warp owns one destination cell; each lane takes one of its sources, so
+//    32 translations run side by side and the destination sum is a reduction
+//    across lanes through shared memory (no atomics, fixed order).
+//  - Expansions of a real field satisfy v_{-m} = (-1)^m conj(v_m); so do all
+//    intermediate vectors (rotations map real fields to real fields). Only
+//    m >= 0 is stored, and each swap matvec splits into two real
+//    (k+1)x(k+1) products: Re(s) = P_k Re(u), Im(s) = Q_k Im(u) with
+//    P_k[r][c] = B_k[r][c] + (-1)^c B_k[r][-c], Q_k[r][c] = B_k[r][c] - (-1)^c B_k[r][-c].
+//  - P_k, Q_k (and those of B_k^T) are pair independent and live in constant
+//    memory; with P fixed at compile time every matrix element is a constant-
+//    bank operand of the FMA that uses it, uniform across the warp.
+//  - Phases e^{imα}, e^{imβ} come from powers of (x + iy)/ρ_xy and
+//    (z + iρ_xy)/R: no trigonometric calls.
+//  - SCALED expansions (mixed form) carry M^_k = M_k / l_a^k and
+//    F^_n = F_n l_b^{n+1}, l the cell's radius, so FP32 never overflows at
+//    high order: the axial kernel becomes (n+k)! (l_a/R)^k (l_b/R)^{n+1}.
+//
+// The including file defines ROTW_T (the element type of the constant tables)
+// before including this header, once per translation unit.
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fmmx {
+
+__host__ __device__ constexpr int rot_hx(int n, int m) { return n * (n + 1) / 2 + m; }
+// offset of degree k's four matrices (P, Q, PT, QT), each (k+1)^2
+__host__ __device__ constexpr int rot_moff(int k) { return 4 * (k * (k + 1) * (2 * k + 1) / 6); }
+#define ROTW_MAXP 16
+#define ROTW_MATS (rot_moff(ROTW_MAXP + 1))
+#define ROTW_NH (rot_hx(ROTW_MAXP, ROTW_MAXP) + 1)
+#define ROTW_LD 33  // entry stride of the per-lane columns (conflict-free both ways)
+
+static __constant__ ROTW_T c_rot[ROTW_MATS];            // P_k, Q_k, P_k^T, Q_k^T per degree
+static __constant__ ROTW_T c_fm[ROTW_NH];               // (n-m)!(n+m)!, half index
+static __constant__ ROTW_T c_ifm[ROTW_NH];              // 1/((n-m)!(n+m)!)
+static __constant__ ROTW_T c_fact[2 * ROTW_MAXP + 1];   // j!
+
+
+// Pair phases e^{imα}, e^{imβ} (m = 0..P): in the lane's shared-memory
+// column (FP64: registers are too few) or in registers (FP32).
+template <typename T>
+struct PhSmem {
+    const cplx<T>* a;
+    const cplx<T>* b;
+    __device__ __forceinline__ cplx<T> A(int m) const { return a[ROTW_LD * m]; }
+    __device__ __forceinline__ cplx<T> B(int m) const { return b[ROTW_LD * m]; }
+};
+template <typename T, int P>
+struct PhRegs {
+    cplx<T> a[P + 1], b[P + 1];
+    __device__ __forceinline__ cplx<T> A(int m) const { return a[m]; }
+    __device__ __forceinline__ cplx<T> B(int m) const { return b[m]; }
+};
+
+template <typename T, int P, bool FULL_LAYOUT, class PH>
+__device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa) {
+    typedef cplx<T> Z;
+    // ---- 1) back-rotation, degree by degree, into this lane's column
+    T sak = T(1);
+#pragma unroll
+    for (int k = 0; k <= P; ++k) {
+        T vr[P + 1], vi[P + 1];
+#pragma unroll
+        for (int m = 0; m <= k; ++m) {
+            const Z M = ms[FULL_LAYOUT ? (k * (k + 1) + m) : rot_hx(k, m)];
+            const Z ph = ph_.A(m);
+            // ph * conj(M), then (-i)^m, then (k-m)!(k+m)!
+            T wr = ph.re * M.re + ph.im * M.im;
+            T wi = ph.im * M.re - ph.re * M.im;
+            T ur, ui;
+            switch (m & 3) {
+                case 0: ur = wr; ui = wi; break;
+                case 1: ur = wi; ui = -wr; break;
+                case 2: ur = -wr; ui = -wi; break;
+                default: ur = -wi; ui = wr; break;
+            }
+            const T f = c_fm[rot_hx(k, m)];
+            vr[m] = ur * f;
+            vi[m] = ui * f;
+        }
+        const T* Pk = c_rot + rot_moff(k);
+        const T* Qk = Pk + (k + 1) * (k + 1);
+        T sr[P + 1], si[P + 1];
+#pragma unroll
+        for (int r = 0; r <= k; ++r) {
+            T a = T(0), b = T(0);
+#pragma unroll
+            for (int q = 0; q <= k; ++q) a += Pk[r * (k + 1) + q] * vr[q];
+#pragma unroll
+            for (int q = 1; q <= k; ++q) b += Qk[r * (k + 1) + q] * vi[q];
+            // q = phb * s
+            const Z pb = ph_.B(r);
+            sr[r] = a * pb.re - b * pb.im;
+            si[r] = a * pb.im + b * pb.re;
+        }
+#pragma unroll
+        for (int r = 0; r <= k; ++r) {
+            T a = T(0), b = T(0);
+#pragma unroll
+            for (int q = 0; q <= k; ++q) a += Pk[r * (k + 1) + q] * sr[q];
+#pragma unroll
+            for (int q = 1; q <= k; ++q) b += Qk[r * (k + 1) + q] * si[q];
+            // b = i^r / fm * t, times the degree scale
+            T orr, oii;
+            switch (r & 3) {
+                case 0: orr = a; oii = b; break;
+                case 1: orr = -b; oii = a; break;
+                case 2: orr = -a; oii = -b; break;
+                default: orr = b; oii = -a; break;
+            }
+            const T g = c_ifm[rot_hx(k, r)] * sak;
+            col[ROTW_LD * rot_hx(k, r)] = mk<T>(orr * g, oii * g);
+        }
+        sak *= sa;
+        // keep degrees apart: bounds the live registers of the unrolled code
+        asm volatile("" ::: "memory");
+    }
+}
+
+template <typename T, int P>
+__device__ __forceinline__ void rotw_axial(cplx<T>* col, T sb) {
+    typedef cplx<T> Z;
+    // ---- 2) axial translation, column by column, in place:
+    // F~[n][m] = (-1)^m conj(sum_{k=m}^{P-n} b[k][m] (n+k)!) sb^{n+1}
+#pragma unroll
+    for (int m = 0; m <= P; ++m) {
+        T br[P + 1], bi[P + 1];
+#pragma unroll
+        for (int k = m; k <= P; ++k) {
+            const Z v = col[ROTW_LD * rot_hx(k, m)];
+            br[k] = v.re;
+            bi[k] = v.im;
+        }
+        T sbn = sb;
+#pragma unroll
+        for (int n = 0; n < m; ++n) sbn *= sb;
+#pragma unroll
+        for (int n = m; n <= P; ++n) {
+            T ar = T(0), ai = T(0);
+#pragma unroll
+            for (int k = m; k <= P - n; ++k) {
+                ar += br[k] * c_fact[n + k];
+                ai += bi[k] * c_fact[n + k];
+            }
+            const T sg = (m & 1) ? T(-1) : T(1);
+            col[ROTW_LD * rot_hx(n, m)] = mk<T>(sg * ar * sbn, -sg * ai * sbn);
+            sbn *= sb;
+        }
+        asm volatile("" ::: "memory");
+    }
+}
+
+template <typename T, int P, class PH>
+__device__ __forceinline__ void rotw_fwd(cplx<T>* col, const PH& ph_) {
+    typedef cplx<T> Z;
+    // ---- 3) forward rotation and scatter into the column
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+        T vr[P + 1], vi[P + 1];
+#pragma unroll
+        for (int m = 0; m <= n; ++m) {
+            const Z F = col[ROTW_LD * rot_hx(n, m)];
+            T ur, ui;  // (-i)^m F / fm
+            switch (m & 3) {
+                case 0: ur = F.re; ui = F.im; break;
+                case 1: ur = F.im; ui = -F.re; break;
+                case 2: ur = -F.re; ui = -F.im; break;
+                default: ur = -F.im; ui = F.re; break;
+            }
+            const T g = c_ifm[rot_hx(n, m)];
+            vr[m] = ur * g;
+            vi[m] = ui * g;
+        }
+        const T* Pt = c_rot + rot_moff(n) + 2 * (n + 1) * (n + 1);
+        const T* Qt = Pt + (n + 1) * (n + 1);
+        T sr[P + 1], si[P + 1];
+#pragma unroll
+        for (int r = 0; r <= n; ++r) {
+            T a = T(0), b = T(0);
+#pragma unroll
+            for (int q = 0; q <= n; ++q) a += Pt[r * (n + 1) + q] * vr[q];
+#pragma unroll
+            for (int q = 1; q <= n; ++q) b += Qt[r * (n + 1) + q] * vi[q];
+            const Z pb = ph_.B(r);  // conj(phb) * s
+            sr[r] = a * pb.re + b * pb.im;
+            si[r] = b * pb.re - a * pb.im;
+        }
+#pragma unroll
+        for (int r = 0; r <= n; ++r) {
+            T a = T(0), b = T(0);
+#pragma unroll
+            for (int q = 0; q <= n; ++q) a += Pt[r * (n + 1) + q] * sr[q];
+#pragma unroll
+            for (int q = 1; q <= n; ++q) b += Qt[r * (n + 1) + q] * si[q];
+            T orr, oii;  // i^r fm * t
+            switch (r & 3) {
+                case 0: orr = a; oii = b; break;
+                case 1: orr = -b; oii = a; break;
+                case 2: orr = -a; oii = -b; break;
+                default: orr = b; oii = -a; break;
+            }
+            const T f = c_fm[rot_hx(n, r)];
+            orr *= f;
+            oii *= f;
+            const Z pa = ph_.A(r);
+            col[ROTW_LD * rot_hx(n, r)] = mk<T>(orr * pa.re - oii * pa.im, orr * pa.im + oii * pa.re);
+        }
+        asm volatile("" ::: "memory");
+    }
+}
+
+// FP64: the three phases are separate non-inlined functions so that each is
+// register-allocated on its own (all three unrolled at once overflow the
+// register file and spill).
+template <typename T, int P, bool FULL_LAYOUT>
+__device__ __noinline__ void rotw_back_ni(const cplx<T>* __restrict__ ms, const cplx<T>* pa, const cplx<T>* pb,
+                                          cplx<T>* col, T sa) {
+    rotw_back<T, P, FULL_LAYOUT>(ms, PhSmem<T>{pa, pb}, col, sa);
+}
+template <typename T, int P>
+__device__ __noinline__ void rotw_axial_ni(cplx<T>* col, T sb) {
+    rotw_axial<T, P>(col, sb);
+}
+template <typename T, int P>
+__device__ __noinline__ void rotw_fwd_ni(cplx<T>* col, const cplx<T>* pa, const cplx<T>* pb) {
+    rotw_fwd<T, P>(col, PhSmem<T>{pa, pb});
+}
+
+template <typename T, int P, bool SCALED, bool FULL_LAYOUT>
+__device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, const uint64_t* __restrict__ keys,
+                                          const CellsView& cv, const T* __restrict__ scale,
+                                          const cplx<T>* __restrict__ mom, cplx<T>* __restrict__ loc,
+                                          cplx<T>* __restrict__ sbuf, int lane) {
+    constexpr int H = (P + 1) * (P + 2) / 2;
+    constexpr int NA = (H + 31) / 32;
+    constexpr int DIM = (P + 1) * (P + 1);
+    typedef cplx<T> Z;
+    constexpr bool PH_REGS = sizeof(T) == 4;
+    Z* col = sbuf + lane;                    // this lane's column: entry e at col[LD e]
+    Z* pha = sbuf + ROTW_LD * H + lane;      // e^{imα}, m = 0..P (FP64 only)
+    Z* phb = pha + ROTW_LD * (P + 1);        // e^{imβ}
+    T acc_re[NA], acc_im[NA];
+#pragma unroll
+    for (int t = 0; t < NA; ++t) acc_re[t] = acc_im[t] = T(0);
+    const double bx = cv.cx[c], by = cv.cy[c], bz = cv.cz[c];
+    for (uint32_t chunk = beg; chunk < end; chunk += 32) {
+        const int nact = (int)min(32u, end - chunk);
+        if (lane < nact) {
+            const int src = (int)(keys[chunk + lane] & 0xffffffffu);
+            // geometry in FP64: r = s_B - z_A
+            const double rx = bx - cv.cx[src], ry = by - cv.cy[src], rz = bz - cv.cz[src];
+            const double rxy2 = rx * rx + ry * ry;
+            const double rxy = sqrt(rxy2);
+            const double R = sqrt(rxy2 + rz * rz);
+            const double iR = 1.0 / R;
+            double ear = 1.0, eai = 0.0;
+            if (rxy > 0.0) {
+                const double ir = 1.0 / rxy;
+                ear = rx * ir;
+                eai = ry * ir;
+            }
+            const T ebr = (T)(rz * iR), ebi = (T)(rxy * iR);
+            PhRegs<T, P> phr;
+            {
+                Z a = mk<T>(T(1), T(0)), b = mk<T>(T(1), T(0));
+                const Z ea = mk<T>((T)ear, (T)eai), eb = mk<T>(ebr, ebi);
+#pragma unroll
+                for (int m = 0; m <= P; ++m) {
+                    if (PH_REGS) {
+                        phr.a[m] = a;
+                        phr.b[m] = b;
+                    } else {
+                        pha[ROTW_LD * m] = a;
+                        phb[ROTW_LD * m] = b;
+                    }
+                    a = zmul(a, ea);
+                    b = zmul(b, eb);
+                }
+            }
+            T sa, sb;  // per-degree scale factors of the axial kernel
+            if (SCALED) {
+                sa = (T)((double)scale[src] * iR);
+                sb = (T)((double)scale[c] * iR);
+            } else {
+                sa = (T)iR;
+                sb = (T)iR;
+            }
+            const Z* ms = mom + (size_t)src * (FULL_LAYOUT ? DIM : H);
+            if constexpr (PH_REGS) {
+                rotw_back<T, P, FULL_LAYOUT>(ms, phr, col, sa);
+                rotw_axial<T, P>(col, sb);
+                rotw_fwd<T, P>(col, phr);
+            } else {
+                rotw_back_ni<T, P, FULL_LAYOUT>(ms, pha, phb, col, sa);
+                rotw_axial_ni<T, P>(col, sb);
+                rotw_fwd_ni<T, P>(col, pha, phb);
+            }
+        }
+        __syncwarp();
+        // ---- 4) destination sum over the chunk's lanes, fixed order
+#pragma unroll
+        for (int t = 0; t < NA; ++t) {
+            const int e = lane + 32 * t;
+            if (e < H) {
+                T sr = T(0), si = T(0);
+                const Z* row = sbuf + ROTW_LD * e;
+                for (int l = 0; l < nact; ++l) {
+                    sr += row[l].re;
+                    si += row[l].im;
+                }
+                acc_re[t] += sr;
+                acc_im[t] += si;
+            }
+        }
+        __syncwarp();
+    }
+    // write the destination's local expansion
+#pragma unroll
+    for (int t = 0; t < NA; ++t) {
+        const int e = lane + 32 * t;
+        if (e < H) {
+            int n = 0;
+            while ((n + 1) * (n + 2) / 2 <= e) ++n;
+            const int m = e - n * (n + 1) / 2;
+            if (FULL_LAYOUT) {
+                cplx<T>* out = loc + (size_t)c * DIM;
+                out[n * (n + 1) + m] = mk<T>(acc_re[t], acc_im[t]);
+                if (m > 0) {
+                    const T sg = (m & 1) ? T(-1) : T(1);
+                    out[n * (n + 1) - m] = mk<T>(sg * acc_re[t], -sg * acc_im[t]);
+                }
+            } else {
+                loc[(size_t)c * H + e] = mk<T>(acc_re[t], acc_im[t]);
+            }
+        }
+    }
+}
+
+template <typename T, int P>
+constexpr size_t rotw_smem_per_warp() {
+    return (size_t)ROTW_LD * ((P + 1) * (P + 2) / 2 + (sizeof(T) == 4 ? 0 : 2 * (P + 1))) * sizeof(cplx<T>);
+}
+
+// Persistent warps pull destination cells from a counter.
+template <typename T, int P, bool SCALED, bool FULL_LAYOUT>
+__global__ void __launch_bounds__(32) k_m2l_rotw(DirList L, int ncells, CellsView cv, const T* __restrict__ scale,
+                                                const cplx<T>* __restrict__ mom, cplx<T>* __restrict__ loc,
+                                                int* __restrict__ work) {
+    extern __shared__ unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw) + (size_t)wib * (rotw_smem_per_warp<T, P>() / sizeof(cplx<T>));
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(work, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= ncells) break;
+        const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
+        if (beg >= end) continue;
+        rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L.keys, cv, scale, mom, loc, sbuf, lane);
+    }
+}
+
+
+}  // namespace fmmx

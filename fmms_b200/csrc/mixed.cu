@@ -1,0 +1,469 @@
+// Mixed-precision form: FP32 expansions and P2P, FP64 only where the reference
+// needs it (centre-relative coordinates, the MAC, M2M/L2L on the top three
+// tree levels).
+//
+// Expansions are stored for m >= 0 only (a real field has
+// v_{-m} = (-1)^m conj(v_m)) and normalised by a per-cell length l (the cell's
+// radius rho, or a small fraction of its box size when rho = 0):
+//     M^_n^m = M_n^m / l^n,      F^_n^m = F_n^m l^{n+1}.
+// Every translation then works on O(1) quantities, so FP32 neither overflows
+// nor underflows at p = 12 for cells down to the level-21 cut:
+//   P2M: M^_n^m  = sum_b m_b Υ_n^m((x_b - s)/l)
+//   M2M: M^_p[n][m] = sum_k sum_l Υ_k^l((s_c - s_p)/l_p) M^_c[n-k][m-l] (l_c/l_p)^{n-k}
+//   L2L: F^_c[n][m] = (l_c/l_p)^{n+1} sum_{k,l} conj(Υ_k^l((s_p - s_c)/l_p)) F^_p[n+k][m+l]
+//   L2P: Ψ_0^0 = (1/l) sum conj(Υ_k^l(r^)) F^_k^l,  Ψ_1^m = (1/l^2) sum conj(Υ_k^l(r^)) F^_{k+1}^{m+l}
+// (the unnormalised forms are moments.rs:30-90 and translate.rs:175-309).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fmmx {
+
+static __constant__ OrderTables c_tab;
+
+void upload_tables_mixed(const OrderTables& t, cudaStream_t s) {
+    cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
+}
+
+__host__ __device__ constexpr int hx(int n, int m) { return n * (n + 1) / 2 + m; }
+
+__device__ __forceinline__ void split_h(int e, int& n, int& m) {
+    int q = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+    while (q * (q + 1) / 2 > e) --q;
+    while ((q + 1) * (q + 2) / 2 <= e) ++q;
+    n = q;
+    m = e - q * (q + 1) / 2;
+}
+
+// v_{n,m} for any m from the half store (m >= 0)
+template <typename T>
+__device__ __forceinline__ cplx<T> half_get(const cplx<T>* v, int n, int m) {
+    if (m >= 0) return v[hx(n, m)];
+    const cplx<T> w = v[hx(n, -m)];
+    return ((-m) & 1) ? mk<T>(-w.re, w.im) : mk<T>(w.re, -w.im);
+}
+
+// Υ column m (harmonic.rs:141-173) of r into u (half layout), precision A.
+template <typename A>
+__device__ __forceinline__ void ups_column(A x, A y, A z, A r2, int p, int m, cplx<A>* u) {
+    cplx<A> d = mk<A>(A(1), A(0));
+    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk<A>(x, y), (A)c_tab.inv2m[j]), d);
+    u[hx(m, m)] = d;
+    cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
+    for (int n = m + 1; n <= p; ++n) {
+        const A a = (A)(2 * n - 1) * z;
+        cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][m]);
+        u[hx(n, m)] = un;
+        u2 = u1;
+        u1 = un;
+    }
+}
+
+// Normalising length of every cell: rho, or side 2^{-level-10} for rho = 0.
+__global__ void k_cell_scale(int nc, const double* __restrict__ rho, const uint8_t* __restrict__ level,
+                             const double* __restrict__ box, double* __restrict__ ell, float* __restrict__ ellf) {
+    const double side = box[6];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        double l = rho[c];
+        if (!(l > 0.0)) l = ldexp(side, -(int)level[c] - 10);
+        ell[c] = l;
+        ellf[c] = (float)l;
+    }
+}
+
+// FP64 full-layout moments (the exact upward pass) -> normalised FP32 half layout.
+__global__ void k_moments_to_mixed(int nc, int p, const zd* __restrict__ full, const double* __restrict__ ell,
+                                   zf* __restrict__ half) {
+    const int H = (p + 1) * (p + 2) / 2, D = (p + 1) * (p + 1);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)nc * H;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / H), e = (int)(i % H);
+        int n, m;
+        split_h(e, n, m);
+        const double s = pow(ell[c], -n);
+        const zd v = full[(size_t)c * D + n * (n + 1) + m];
+        half[i] = mk<float>((float)(v.re * s), (float)(v.im * s));
+    }
+}
+
+// P2M / M2M for one level, one warp per cell. A = accumulation type (double
+// on the top three levels, float below). Output FP32 half layout.
+template <typename A>
+__global__ void k_upward_mixed(const int32_t* __restrict__ level_cells, int lstart, int lcnt, CellsView cv,
+                               const double* __restrict__ ell, const double* __restrict__ x,
+                               const double* __restrict__ y, const double* __restrict__ z,
+                               const double* __restrict__ m, int p, zf* __restrict__ mom) {
+    extern __shared__ unsigned char smem_raw[];
+    const int H = (p + 1) * (p + 2) / 2;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw) + (size_t)wib * 2 * H;
+    cplx<A>* acc = u + H;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int j = warp; j < lcnt; j += nwarps) {
+        const int c = level_cells[lstart + j];
+        const double sx = cv.cx[c], sy = cv.cy[c], sz = cv.cz[c];
+        const double il = 1.0 / ell[c];
+        for (int e = lane; e < H; e += 32) acc[e] = mk<A>(A(0), A(0));
+        __syncwarp();
+        if (cv.leaf[c]) {
+            // lanes over bodies, each with its own Υ table column set: lane
+            // handles body b, all columns; sums into acc by warp reduction per entry
+            const uint32_t f = cv.first[c], cnt = cv.count[c];
+            for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
+                const uint32_t b = b0 + lane;
+                const bool act = b < cnt;
+                A rx = 0, ry = 0, rz = 0, mb = 0;
+                if (act) {
+                    rx = (A)((x[f + b] - sx) * il);
+                    ry = (A)((y[f + b] - sy) * il);
+                    rz = (A)((z[f + b] - sz) * il);
+                    mb = (A)m[f + b];
+                }
+                const A r2 = rx * rx + ry * ry + rz * rz;
+                cplx<A> d = mk<A>(A(1), A(0));
+                for (int mm = 0; mm <= p; ++mm) {
+                    if (mm > 0) d = zmul(zscale(mk<A>(rx, ry), (A)c_tab.inv2m[mm]), d);
+                    cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
+                    for (int n = mm; n <= p; ++n) {
+                        cplx<A> un;
+                        if (n == mm) {
+                            un = d;
+                        } else {
+                            const A a = (A)(2 * n - 1) * rz;
+                            un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][mm]);
+                            u2 = u1;
+                            u1 = un;
+                        }
+                        A vr = un.re * mb, vi = un.im * mb;
+                        for (int o = 16; o > 0; o >>= 1) {
+                            vr += __shfl_xor_sync(0xffffffffu, vr, o);
+                            vi += __shfl_xor_sync(0xffffffffu, vi, o);
+                        }
+                        if (lane == 0) {
+                            acc[hx(n, mm)].re += vr;
+                            acc[hx(n, mm)].im += vi;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        } else {
+            for (int o = 0; o < 8; ++o) {
+                const int ch = cv.child[8 * c + o];
+                if (ch < 0) continue;
+                const A dx = (A)((cv.cx[ch] - sx) * il), dy = (A)((cv.cy[ch] - sy) * il),
+                        dz = (A)((cv.cz[ch] - sz) * il);
+                const A r2 = dx * dx + dy * dy + dz * dz;
+                for (int mm = lane; mm <= p; mm += 32) ups_column<A>(dx, dy, dz, r2, p, mm, u);
+                __syncwarp();
+                const A ratio = (A)(ell[ch] * il);
+                const zf* mc = mom + (size_t)ch * H;
+                for (int e = lane; e < H; e += 32) {
+                    int n, mm;
+                    split_h(e, n, mm);
+                    A sr = 0, si = 0;
+                    A rpow = 1;  // ratio^{n-k}, built from k = n down
+                    for (int k = n; k >= 0; --k) {
+                        const int nk = n - k;
+                        const int lo = max(-k, mm - nk), hi = min(k, mm + nk);
+                        A tr = 0, ti = 0;
+                        for (int l = lo; l <= hi; ++l) {
+                            const cplx<A> uu = half_get<A>(u, k, l);
+                            const zf mv = half_get<float>(mc, nk, mm - l);
+                            tr += uu.re * (A)mv.re - uu.im * (A)mv.im;
+                            ti += uu.re * (A)mv.im + uu.im * (A)mv.re;
+                        }
+                        sr += tr * rpow;
+                        si += ti * rpow;
+                        rpow *= ratio;
+                    }
+                    acc[e].re += sr;
+                    acc[e].im += si;
+                }
+                __syncwarp();
+            }
+        }
+        zf* out = mom + (size_t)c * H;
+        for (int e = lane; e < H; e += 32) out[e] = mk<float>((float)acc[e].re, (float)acc[e].im);
+        __syncwarp();
+    }
+}
+
+void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
+                         int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,
+                         const double* z, const double* m, int p, zf* mom) {
+    const int H = (p + 1) * (p + 2) / 2;
+    if (fp64)
+        k_upward_mixed<double><<<grid, 32 * warps, (size_t)warps * 2 * H * sizeof(zd), s>>>(
+            level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+    else
+        k_upward_mixed<float><<<grid, 32 * warps, (size_t)warps * 2 * H * sizeof(zf), s>>>(
+            level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+}
+
+// L2L for the cells of one level (L >= 1), one CTA per cell; A as above.
+template <typename A>
+__global__ void __launch_bounds__(128) k_l2l_mixed(const int32_t* __restrict__ level_cells, int lstart, int lcnt,
+                                                  CellsView cv, const int32_t* __restrict__ parent,
+                                                  const double* __restrict__ ell, int p, zf* __restrict__ loc) {
+    extern __shared__ unsigned char smem_raw[];
+    const int H = (p + 1) * (p + 2) / 2;
+    cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw);
+    zf* fp = reinterpret_cast<zf*>(u + H);
+    const int tid = threadIdx.x;
+    for (int j = blockIdx.x; j < lcnt; j += gridDim.x) {
+        const int c = level_cells[lstart + j];
+        const int par = parent[c];
+        if (par < 0) continue;
+        const double il = 1.0 / ell[par];
+        const A rx = (A)((cv.cx[par] - cv.cx[c]) * il), ry = (A)((cv.cy[par] - cv.cy[c]) * il),
+                rz = (A)((cv.cz[par] - cv.cz[c]) * il);
+        if (tid <= p) ups_column<A>(rx, ry, rz, rx * rx + ry * ry + rz * rz, p, tid, u);
+        const zf* lp = loc + (size_t)par * H;
+        for (int e = tid; e < H; e += blockDim.x) fp[e] = lp[e];
+        __syncthreads();
+        const A ratio = (A)(ell[c] * il);
+        zf* lc = loc + (size_t)c * H;
+        for (int e = tid; e < H; e += blockDim.x) {
+            int n, m;
+            split_h(e, n, m);
+            A sr = 0, si = 0;
+            for (int k = 0; k <= p - n; ++k) {
+                for (int l = -k; l <= k; ++l) {
+                    const cplx<A> a = half_get<A>(u, k, l);
+                    const zf b = half_get<float>(fp, n + k, m + l);
+                    sr += a.re * (A)b.re + a.im * (A)b.im;  // conj(a) * b
+                    si += a.re * (A)b.im - a.im * (A)b.re;
+                }
+            }
+            A sc = ratio;
+            for (int q = 0; q < n; ++q) sc *= ratio;
+            const zf cur = lc[e];
+            lc[e] = mk<float>((float)((A)cur.re + sr * sc), (float)((A)cur.im + si * sc));
+        }
+        __syncthreads();
+    }
+}
+
+void launch_l2l_mixed(bool fp64, unsigned grid, cudaStream_t s, const int32_t* level_cells, int lstart, int lcnt,
+                      CellsView cv, const int32_t* parent, const double* ell, int p, zf* loc) {
+    const int H = (p + 1) * (p + 2) / 2;
+    if (fp64)
+        k_l2l_mixed<double><<<grid, 128, H * (sizeof(zd) + sizeof(zf)), s>>>(level_cells, lstart, lcnt, cv, parent,
+                                                                           ell, p, loc);
+    else
+        k_l2l_mixed<float><<<grid, 128, H * (sizeof(zf) + sizeof(zf)), s>>>(level_cells, lstart, lcnt, cv, parent,
+                                                                          ell, p, loc);
+}
+
+// L2P at every body plus the near field, scattered to particle-id order.
+__global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, const uint32_t* __restrict__ order,
+                            CellsView cv, const double* __restrict__ ell, int p, const zf* __restrict__ loc,
+                            const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const double* __restrict__ nax,
+                            const double* __restrict__ nay, const double* __restrict__ naz,
+                            const double* __restrict__ npot, double* __restrict__ acc, double* __restrict__ pot) {
+    const int H = (p + 1) * (p + 2) / 2;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int c = body_leaf[k];
+        const double l = ell[c], il = 1.0 / l;
+        const float rx = (float)((cv.cx[c] - x[k]) * il), ry = (float)((cv.cy[c] - y[k]) * il),
+                    rz = (float)((cv.cz[c] - z[k]) * il);
+        const float r2 = rx * rx + ry * ry + rz * rz;
+        const zf* L = loc + (size_t)c * H;
+        float p00 = 0, p11r = 0, p11i = 0, p10 = 0;
+        zf d = mk<float>(1.f, 0.f);
+        for (int lm = 0; lm <= p; ++lm) {
+            if (lm > 0) d = zmul(zscale(mk<float>(rx, ry), (float)c_tab.inv2m[lm]), d);
+            zf u1 = d, u2 = mk<float>(0.f, 0.f);
+            const float sgn = (lm & 1) ? -1.f : 1.f;
+            for (int kk = lm; kk <= p; ++kk) {
+                zf uk;
+                if (kk == lm) {
+                    uk = d;
+                } else {
+                    const float a = (float)(2 * kk - 1) * rz;
+                    uk = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (float)c_tab.invc[kk][lm]);
+                    u2 = u1;
+                    u1 = uk;
+                }
+                const zf f0 = L[hx(kk, lm)];
+                p00 += uk.re * f0.re + uk.im * f0.im;
+                if (kk < p) {
+                    const zf f11 = half_get<float>(L, kk + 1, lm + 1);
+                    const zf f10 = L[hx(kk + 1, lm)];
+                    p11r += uk.re * f11.re + uk.im * f11.im;
+                    p11i += uk.re * f11.im - uk.im * f11.re;
+                    p10 += uk.re * f10.re + uk.im * f10.im;
+                }
+                if (lm > 0) {
+                    const zf g0 = half_get<float>(L, kk, -lm);
+                    p00 += sgn * (uk.re * g0.re - uk.im * g0.im);
+                    if (kk < p) {
+                        const zf g11 = half_get<float>(L, kk + 1, 1 - lm);
+                        const zf g10 = half_get<float>(L, kk + 1, -lm);
+                        p11r += sgn * (uk.re * g11.re - uk.im * g11.im);
+                        p11i += sgn * (uk.re * g11.im + uk.im * g11.re);
+                        p10 += sgn * (uk.re * g10.re - uk.im * g10.im);
+                    }
+                }
+            }
+        }
+        const double s1 = il, s2 = il * il;
+        const uint32_t id = order[k];
+        acc[3 * (size_t)id + 0] = nax[k] - (double)p11r * s2;
+        acc[3 * (size_t)id + 1] = nay[k] - (double)p11i * s2;
+        acc[3 * (size_t)id + 2] = naz[k] - (double)p10 * s2;
+        pot[id] = npot[k] + (double)p00 * s1;
+    }
+}
+
+// ------------------------------------------------------------------ P2P
+// FP32 P2P with compensated accumulation. Source bodies are staged in shared
+// memory relative to the target leaf's centre (the FP64 subtraction), so the
+// FP32 differences d = x_j - x_i keep their relative precision; each thread
+// sums a tile in FP32 and adds the tile's partial into a double-single
+// (hi, lo) accumulator with an error-free TwoSum. 1/r by rsqrt plus one
+// Newton step.
+#define P2PM_BLOCK 128
+#define P2PM_TILE 256
+#define P2PM_SRC_CHUNK 256
+
+struct DS {
+    float hi, lo;
+};
+__device__ __forceinline__ void ds_add(DS& a, float b) {
+    const float s = a.hi + b;
+    const float bb = s - a.hi;
+    const float err = (a.hi - (s - bb)) + (b - bb);
+    a.hi = s;
+    a.lo += err;
+}
+
+__global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv,
+                                                         const double* __restrict__ x, const double* __restrict__ y,
+                                                         const double* __restrict__ z, const double* __restrict__ m,
+                                                         float soft2, double* __restrict__ ax,
+                                                         double* __restrict__ ay, double* __restrict__ az,
+                                                         double* __restrict__ pot) {
+    __shared__ float4 tb[P2PM_TILE];  // x, y, z relative to the target centre; mass
+    __shared__ uint32_t tslot[P2PM_TILE];
+    __shared__ uint32_t pre[P2PM_SRC_CHUNK + 1];
+    __shared__ uint32_t sfirst[P2PM_SRC_CHUNK];
+    __shared__ float red[8][P2PM_BLOCK];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
+    for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+        const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
+        if (beg >= end) continue;
+        const double cx = cv.cx[c], cy = cv.cy[c], cz = cv.cz[c];
+        const uint32_t tf = cv.first[c], tn = cv.count[c];
+        for (uint32_t t0 = 0; t0 < tn; t0 += P2PM_BLOCK) {
+            const int nt = (int)min((uint32_t)P2PM_BLOCK, tn - t0);
+            const int R = P2PM_BLOCK / nt;
+            const int it = tid % nt, rep = tid / nt;
+            const bool active = rep < R;
+            const uint32_t islot = tf + t0 + it;
+            float xi = 0, yi = 0, zi = 0;
+            if (active) {
+                xi = (float)(x[islot] - cx);
+                yi = (float)(y[islot] - cy);
+                zi = (float)(z[islot] - cz);
+            }
+            DS sax{0, 0}, say{0, 0}, saz{0, 0}, sp{0, 0};
+            for (uint32_t sc = beg; sc < end; sc += P2PM_SRC_CHUNK) {
+                const int ns = (int)min((uint32_t)P2PM_SRC_CHUNK, end - sc);
+                __syncthreads();
+                // exclusive prefix of source leaf sizes (warp scans, then warp totals)
+                for (int q0 = 0; q0 < ns; q0 += P2PM_BLOCK) {
+                    const int q = q0 + tid;
+                    uint32_t v = 0;
+                    if (q < ns) {
+                        const int src = (int)(L.keys[sc + q] & 0xffffffffu);
+                        v = cv.count[src];
+                        sfirst[q] = cv.first[src];
+                    }
+                    uint32_t incl = v;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    __shared__ uint32_t wsum[P2PM_BLOCK / 32];
+                    if (lane == 31) wsum[wid] = incl;
+                    __syncthreads();
+                    uint32_t base = q0 == 0 ? 0 : pre[q0];
+                    for (int w = 0; w < wid; ++w) base += wsum[w];
+                    if (q < ns) pre[q + 1] = base + incl;
+                    if (q0 == 0 && tid == 0) pre[0] = 0;
+                    __syncthreads();
+                }
+                const uint32_t total = pre[ns];
+                for (uint32_t b0 = 0; b0 < total; b0 += P2PM_TILE) {
+                    const uint32_t nb = min((uint32_t)P2PM_TILE, total - b0);
+                    for (uint32_t t = tid; t < nb; t += P2PM_BLOCK) {
+                        const uint32_t g = b0 + t;
+                        int lo = 0, hi = ns;
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (pre[mid] <= g) lo = mid;
+                            else hi = mid;
+                        }
+                        const uint32_t slot = sfirst[lo] + (g - pre[lo]);
+                        tb[t] = make_float4((float)(x[slot] - cx), (float)(y[slot] - cy), (float)(z[slot] - cz),
+                                            (float)m[slot]);
+                        tslot[t] = slot;
+                    }
+                    __syncthreads();
+                    if (active) {
+                        float pax = 0.f, pay = 0.f, paz = 0.f, pp = 0.f;
+                        for (uint32_t j = rep; j < nb; j += R) {
+                            const float4 s = tb[j];
+                            const float dx = s.x - xi, dy = s.y - yi, dz = s.z - zi;
+                            const bool self = tslot[j] == islot;  // the target itself: no term
+                            const float r2 = self ? 1.f : fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+                            float inv = rsqrtf(r2);
+                            inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
+                            const float mj = self ? 0.f : s.w;
+                            const float mi = mj * inv;
+                            const float f = mi * inv * inv;
+                            pax = fmaf(f, dx, pax);
+                            pay = fmaf(f, dy, pay);
+                            paz = fmaf(f, dz, paz);
+                            pp += mi;
+                        }
+                        ds_add(sax, pax);
+                        ds_add(say, pay);
+                        ds_add(saz, paz);
+                        ds_add(sp, pp);
+                    }
+                    __syncthreads();
+                }
+            }
+            red[0][tid] = sax.hi;
+            red[1][tid] = sax.lo;
+            red[2][tid] = say.hi;
+            red[3][tid] = say.lo;
+            red[4][tid] = saz.hi;
+            red[5][tid] = saz.lo;
+            red[6][tid] = sp.hi;
+            red[7][tid] = sp.lo;
+            __syncthreads();
+            if (tid < nt) {
+                double s[4] = {0, 0, 0, 0};
+                for (int r = 0; r < R; ++r) {
+                    const int q = r * nt + tid;
+                    for (int k = 0; k < 4; ++k) s[k] += (double)red[2 * k][q] + (double)red[2 * k + 1][q];
+                }
+                const uint32_t slot = tf + t0 + tid;
+                ax[slot] = s[0];
+                ay[slot] = s[1];
+                az[slot] = s[2];
+                pot[slot] = s[3];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace fmmx

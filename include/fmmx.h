@@ -52,8 +52,11 @@ typedef enum fmmx_center_mode { FMMX_CENTER_COM = 0, FMMX_CENTER_SPHERE = 1 } fm
  * for centre-relative subtraction, the MAC, and M2M/L2L on the top 3 levels. */
 typedef enum fmmx_precision { FMMX_PLAIN_FP64 = 0, FMMX_MIXED = 1 } fmmx_precision;
 
-/* M2L kernel. AUTO follows the reference rule (naive below p = 20, rotation
- * from p = 20, rotation.rs:45 and fmm.rs:90-94). */
+/* M2L kernel. NAIVE is the reference's O(p^4) convolution (translate.rs:47-136);
+ * ROTATION the O(p^3) rotate / translate-along-z / rotate-back kernel
+ * (rotation.rs:262-435). AUTO picks the faster on the device, which is the
+ * rotation kernel at every p (the reference switches to rotation only from
+ * p = 20, rotation.rs:45, because on its CPU the naive form wins below). */
 typedef enum fmmx_m2l_kernel { FMMX_M2L_AUTO = 0, FMMX_M2L_NAIVE = 1, FMMX_M2L_ROTATION = 2 } fmmx_m2l_kernel;
 
 typedef struct fmmx_config {
@@ -89,6 +92,7 @@ typedef struct fmmx_stats {
     double ms_l2l;
     double ms_l2p;
     double ms_evaluate;        /* whole evaluate, device time */
+    uint64_t kernel_launches;  /* engine kernels launched by the last build + evaluate */
 } fmmx_stats;
 
 typedef struct fmmx_ctx fmmx_ctx;
@@ -157,12 +161,33 @@ fmmx_status fmmx_export_expansions(const fmmx_ctx* ctx, double* moments, double*
 fmmx_status fmmx_direct_targets(int device, size_t n, const double* pos_xyz, const double* mass, double softening,
                                 size_t nt, const uint32_t* targets, double* acc_xyz, double* pot, double* fscale);
 
+/* Diagnostics: measured FMA throughput of this device in TFLOP/s (an FMA
+ * counts 2 flops) for FP64 (fp64 != 0) or FP32, from a register-resident FMA
+ * loop over every SM. The roofline denominator of the CUDA-core kernels. No
+ * reference counterpart. */
+fmmx_status fmmx_probe_fma_peak(int device, int fp64, double* tflops);
+
 /* ------------------------------------------------------------------ generators
  * Seeded inputs, host side. fmmx_gen_plummer reproduces models::plummer
  * (models.rs:35-58) bit for bit; fmmx_gen_hernquist models::hernquist
  * (models.rs:61-82). */
 void fmmx_gen_plummer(size_t n, double cx, double cy, double cz, uint64_t seed, double* mass, double* pos_xyz);
 void fmmx_gen_hernquist(size_t n, double cx, double cy, double cz, uint64_t seed, double* mass, double* pos_xyz);
+
+/* Benchmark workloads (extensions, no reference counterpart).
+ * fmmx_gen_plummer_ic: Plummer sphere (mass mtot, scale a) truncated at
+ *   r <= rmax*a, isotropic velocities from the Plummer distribution function
+ *   (vel n x 3, nullable).
+ * fmmx_gen_uniform_lognormal: uniform in the unit cube, masses exp(N(0,sigma^2))
+ *   normalised to sum 1.
+ * fmmx_gen_clusters: nclust Plummer spheres, scale radii log-uniform in
+ *   [amin, amax], centres uniform in the unit cube, sizes a Dirichlet(1) split
+ *   of n, equal masses summing to 1. */
+void fmmx_gen_plummer_ic(size_t n, double mtot, double a, double rmax, uint64_t seed, double* mass, double* pos_xyz,
+                         double* vel_xyz);
+void fmmx_gen_uniform_lognormal(size_t n, double sigma, uint64_t seed, double* mass, double* pos_xyz);
+void fmmx_gen_clusters(size_t n, int nclust, double amin, double amax, uint64_t seed, double* mass, double* pos_xyz,
+                       double* vel_xyz);
 
 #ifdef __cplusplus
 }
