@@ -121,6 +121,7 @@ SIGNATURES = {
     "fmmx_export_expansions": (_st, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "fmmx_direct_targets": (_st, [C.c_int, _sz, _dp, _dp, C.c_double, _sz, _u32p, _dp, _dp, _dp]),
     "fmmx_probe_fma_peak": (_st, [C.c_int, C.c_int, _dp]),
+    "fmmx_direct_targets_noalloc": (_st, [C.c_int, _vp, _sz, _vp, _vp, C.c_double, _sz, _vp, _vp, _vp, _vp]),
     "fmmx_gen_plummer": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]),
     "fmmx_gen_hernquist": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]),
     "fmmx_gen_plummer_ic": (None, [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp, _dp]),
@@ -377,3 +378,16 @@ def probe_fma_peak(fp64: bool, device: int = 0) -> float:
     if st != 0:
         raise FmmError(st, "fmmx_probe_fma_peak failed")
     return out.value
+
+
+DIRECT_NOALLOC_MAX_TARGETS = 4096
+
+
+def direct_targets_noalloc(n, d_pos, d_mass, nt, d_targets, d_acc, d_pot=None, d_fscale=None, softening=0.0,
+                           device=0, stream=None):
+    """Allocation-free direct sum on device buffers (integer device pointers);
+    queued on `stream`, returns without waiting. See fmmx_direct_targets_noalloc."""
+    st = lib().fmmx_direct_targets_noalloc(device, stream, n, d_pos, d_mass, float(softening), nt, d_targets,
+                                           d_acc, d_pot, d_fscale)
+    if st != 0:
+        raise FmmError(st, "fmmx_direct_targets_noalloc failed")

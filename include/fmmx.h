@@ -161,6 +161,24 @@ fmmx_status fmmx_export_expansions(const fmmx_ctx* ctx, double* moments, double*
 fmmx_status fmmx_direct_targets(int device, size_t n, const double* pos_xyz, const double* mass, double softening,
                                 size_t nt, const uint32_t* targets, double* acc_xyz, double* pot, double* fscale);
 
+/* Allocation-free form of fmmx_direct_targets, with no counterpart in the
+ * reference: for callers that cannot allocate device memory, such as a physics
+ * step in a fixed-latency frame loop (cudaMalloc/cudaFree can block and
+ * synchronise the device) or a host whose device memory is owned by its own
+ * pool allocator. All pointers are device memory of `device`; work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream) and the call returns
+ * without waiting. The per-split partial sums live in a static device array
+ * sized for nt <= FMMX_DIRECT_NOALLOC_MAX_TARGETS (about 5 MB, held by every
+ * GPU that loads the library until exit); larger nt returns FMMX_INVALID_ARG.
+ * The first call on a device looks up that array's address, so make it before
+ * any stream capture. Calls share the array: calls that overlap on the GPU
+ * race. A target id >= n yields NaN for that target. */
+#define FMMX_DIRECT_NOALLOC_MAX_TARGETS 4096
+fmmx_status fmmx_direct_targets_noalloc(int device, void* stream, size_t n, const double* d_pos_xyz,
+                                        const double* d_mass, double softening, size_t nt,
+                                        const uint32_t* d_targets, double* d_acc_xyz, double* d_pot,
+                                        double* d_fscale);
+
 /* Diagnostics: measured FMA throughput of this device in TFLOP/s (an FMA
  * counts 2 flops) for FP64 (fp64 != 0) or FP32, from a register-resident FMA
  * loop over every SM. The roofline denominator of the CUDA-core kernels. No
