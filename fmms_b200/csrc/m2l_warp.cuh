@@ -30,6 +30,9 @@
 // before including this header, once per translation unit.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -65,161 +68,190 @@ struct PhRegs {
     __device__ __forceinline__ cplx<T> B(int m) const { return b[m]; }
 };
 
+// The per-degree (per-column) bodies below take the degree as a template
+// parameter and are expanded over 0..P with an index_sequence fold, so every
+// matrix offset, loop bound and array index is a compile-time constant and the
+// swap-matrix elements reach the FMAs as constant-bank operands.
+
+// (-i)^m * (ur + i ui) for m mod 4, and i^m * (...)
+template <int M, typename T>
+__device__ __forceinline__ void mul_mi_pow(T& r, T& i) {
+    const T a = r, b = i;
+    if constexpr ((M & 3) == 1) { r = b; i = -a; }
+    else if constexpr ((M & 3) == 2) { r = -a; i = -b; }
+    else if constexpr ((M & 3) == 3) { r = -b; i = a; }
+}
+template <int M, typename T>
+__device__ __forceinline__ void mul_i_pow(T& r, T& i) {
+    const T a = r, b = i;
+    if constexpr ((M & 3) == 1) { r = -b; i = a; }
+    else if constexpr ((M & 3) == 2) { r = -a; i = -b; }
+    else if constexpr ((M & 3) == 3) { r = b; i = -a; }
+}
+
+// Real half-basis swap matvec: Re(s) = Pm Re(v), Im(s) = Qm Im(v).
+template <typename T, int N, int OFF>
+__device__ __forceinline__ void swap_matvec(const T (&vr)[N], const T (&vi)[N], T (&sr)[N], T (&si)[N]) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+        T a = c_rot[OFF + r * N] * vr[0];
+        T b = T(0);
+#pragma unroll
+        for (int q = 1; q < N; ++q) {
+            a += c_rot[OFF + r * N + q] * vr[q];
+            b += c_rot[OFF + N * N + r * N + q] * vi[q];
+        }
+        sr[r] = a;
+        si[r] = b;
+    }
+}
+
+template <int M, typename T, int N>
+struct Unroll {  // compile-time loop helper: f(integral_constant<m>) for m = M..N-1
+    template <class F>
+    __device__ __forceinline__ static void run(F&& f) {
+        if constexpr (M < N) {
+            f(std::integral_constant<int, M>{});
+            Unroll<M + 1, T, N>::run(f);
+        }
+    }
+};
+
+template <typename T, int P, int K, bool FULL_LAYOUT, class PH>
+__device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,
+                                            T& sak) {
+    typedef cplx<T> Z;
+    constexpr int N = K + 1;
+    T vr[N], vi[N];
+    Unroll<0, T, N>::run([&](auto mc) {
+        constexpr int m = decltype(mc)::value;
+        const Z M = ms[FULL_LAYOUT ? (K * (K + 1) + m) : rot_hx(K, m)];
+        const Z ph = ph_.A(m);
+        T ur = ph.re * M.re + ph.im * M.im;  // ph * conj(M)
+        T ui = ph.im * M.re - ph.re * M.im;
+        mul_mi_pow<m>(ur, ui);
+        const T f = c_fm[rot_hx(K, m)];
+        vr[m] = ur * f;
+        vi[m] = ui * f;
+    });
+    T sr[N], si[N];
+    swap_matvec<T, N, rot_moff(K)>(vr, vi, sr, si);
+    Unroll<0, T, N>::run([&](auto rc) {  // q = phb * s
+        constexpr int r = decltype(rc)::value;
+        const Z pb = ph_.B(r);
+        const T a = sr[r], b = si[r];
+        vr[r] = a * pb.re - b * pb.im;
+        vi[r] = a * pb.im + b * pb.re;
+    });
+    swap_matvec<T, N, rot_moff(K)>(vr, vi, sr, si);
+    Unroll<0, T, N>::run([&](auto rc) {  // b = i^r / fm * t * sa^k
+        constexpr int r = decltype(rc)::value;
+        T orr = sr[r], oii = si[r];
+        mul_i_pow<r>(orr, oii);
+        const T g = c_ifm[rot_hx(K, r)] * sak;
+        col[ROTW_LD * rot_hx(K, r)] = mk<T>(orr * g, oii * g);
+    });
+    sak *= sa;
+    asm volatile("" ::: "memory");  // keep degrees apart: bounds the live registers
+}
+
+template <typename T, int P, bool FULL_LAYOUT, class PH, int... Ks>
+__device__ __forceinline__ void back_all(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,
+                                         std::integer_sequence<int, Ks...>) {
+    T sak = T(1);
+    (back_degree<T, P, Ks, FULL_LAYOUT, PH>(ms, ph_, col, sa, sak), ...);
+}
+
 template <typename T, int P, bool FULL_LAYOUT, class PH>
 __device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa) {
-    typedef cplx<T> Z;
-    // ---- 1) back-rotation, degree by degree, into this lane's column
-    T sak = T(1);
+    back_all<T, P, FULL_LAYOUT, PH>(ms, ph_, col, sa, std::make_integer_sequence<int, P + 1>{});
+}
+
+// axial translation of column m, in place:
+// F~[n][m] = (-1)^m conj(sum_{k=m}^{P-n} b[k][m] (n+k)!) sb^{n+1}
+template <typename T, int P, int M>
+__device__ __forceinline__ void axial_col(cplx<T>* col, T sb) {
+    constexpr int L = P - M + 1;  // entries k = M..P
+    T br[L], bi[L];
+    Unroll<0, T, L>::run([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        const cplx<T> v = col[ROTW_LD * rot_hx(M + j, M)];
+        br[j] = v.re;
+        bi[j] = v.im;
+    });
+    T sbn = sb;
 #pragma unroll
-    for (int k = 0; k <= P; ++k) {
-        T vr[P + 1], vi[P + 1];
-#pragma unroll
-        for (int m = 0; m <= k; ++m) {
-            const Z M = ms[FULL_LAYOUT ? (k * (k + 1) + m) : rot_hx(k, m)];
-            const Z ph = ph_.A(m);
-            // ph * conj(M), then (-i)^m, then (k-m)!(k+m)!
-            T wr = ph.re * M.re + ph.im * M.im;
-            T wi = ph.im * M.re - ph.re * M.im;
-            T ur, ui;
-            switch (m & 3) {
-                case 0: ur = wr; ui = wi; break;
-                case 1: ur = wi; ui = -wr; break;
-                case 2: ur = -wr; ui = -wi; break;
-                default: ur = -wi; ui = wr; break;
-            }
-            const T f = c_fm[rot_hx(k, m)];
-            vr[m] = ur * f;
-            vi[m] = ui * f;
-        }
-        const T* Pk = c_rot + rot_moff(k);
-        const T* Qk = Pk + (k + 1) * (k + 1);
-        T sr[P + 1], si[P + 1];
-#pragma unroll
-        for (int r = 0; r <= k; ++r) {
-            T a = T(0), b = T(0);
-#pragma unroll
-            for (int q = 0; q <= k; ++q) a += Pk[r * (k + 1) + q] * vr[q];
-#pragma unroll
-            for (int q = 1; q <= k; ++q) b += Qk[r * (k + 1) + q] * vi[q];
-            // q = phb * s
-            const Z pb = ph_.B(r);
-            sr[r] = a * pb.re - b * pb.im;
-            si[r] = a * pb.im + b * pb.re;
-        }
-#pragma unroll
-        for (int r = 0; r <= k; ++r) {
-            T a = T(0), b = T(0);
-#pragma unroll
-            for (int q = 0; q <= k; ++q) a += Pk[r * (k + 1) + q] * sr[q];
-#pragma unroll
-            for (int q = 1; q <= k; ++q) b += Qk[r * (k + 1) + q] * si[q];
-            // b = i^r / fm * t, times the degree scale
-            T orr, oii;
-            switch (r & 3) {
-                case 0: orr = a; oii = b; break;
-                case 1: orr = -b; oii = a; break;
-                case 2: orr = -a; oii = -b; break;
-                default: orr = b; oii = -a; break;
-            }
-            const T g = c_ifm[rot_hx(k, r)] * sak;
-            col[ROTW_LD * rot_hx(k, r)] = mk<T>(orr * g, oii * g);
-        }
-        sak *= sa;
-        // keep degrees apart: bounds the live registers of the unrolled code
-        asm volatile("" ::: "memory");
-    }
+    for (int n = 0; n < M; ++n) sbn *= sb;
+    constexpr T sg = (M & 1) ? T(-1) : T(1);
+    Unroll<M, T, P + 1>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        T ar = T(0), ai = T(0);
+        Unroll<M, T, P - n + 1>::run([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            ar += br[k - M] * c_fact[n + k];
+            ai += bi[k - M] * c_fact[n + k];
+        });
+        col[ROTW_LD * rot_hx(n, M)] = mk<T>(sg * ar * sbn, -sg * ai * sbn);
+        sbn *= sb;
+    });
+    asm volatile("" ::: "memory");
+}
+
+template <typename T, int P, int... Ms>
+__device__ __forceinline__ void axial_all(cplx<T>* col, T sb, std::integer_sequence<int, Ms...>) {
+    (axial_col<T, P, Ms>(col, sb), ...);
 }
 
 template <typename T, int P>
 __device__ __forceinline__ void rotw_axial(cplx<T>* col, T sb) {
+    axial_all<T, P>(col, sb, std::make_integer_sequence<int, P + 1>{});
+}
+
+template <typename T, int P, int K, class PH>
+__device__ __forceinline__ void fwd_degree(cplx<T>* col, const PH& ph_) {
     typedef cplx<T> Z;
-    // ---- 2) axial translation, column by column, in place:
-    // F~[n][m] = (-1)^m conj(sum_{k=m}^{P-n} b[k][m] (n+k)!) sb^{n+1}
-#pragma unroll
-    for (int m = 0; m <= P; ++m) {
-        T br[P + 1], bi[P + 1];
-#pragma unroll
-        for (int k = m; k <= P; ++k) {
-            const Z v = col[ROTW_LD * rot_hx(k, m)];
-            br[k] = v.re;
-            bi[k] = v.im;
-        }
-        T sbn = sb;
-#pragma unroll
-        for (int n = 0; n < m; ++n) sbn *= sb;
-#pragma unroll
-        for (int n = m; n <= P; ++n) {
-            T ar = T(0), ai = T(0);
-#pragma unroll
-            for (int k = m; k <= P - n; ++k) {
-                ar += br[k] * c_fact[n + k];
-                ai += bi[k] * c_fact[n + k];
-            }
-            const T sg = (m & 1) ? T(-1) : T(1);
-            col[ROTW_LD * rot_hx(n, m)] = mk<T>(sg * ar * sbn, -sg * ai * sbn);
-            sbn *= sb;
-        }
-        asm volatile("" ::: "memory");
-    }
+    constexpr int N = K + 1;
+    T vr[N], vi[N];
+    Unroll<0, T, N>::run([&](auto mc) {  // g = (-i)^m F / fm
+        constexpr int m = decltype(mc)::value;
+        const Z F = col[ROTW_LD * rot_hx(K, m)];
+        T ur = F.re, ui = F.im;
+        mul_mi_pow<m>(ur, ui);
+        const T g = c_ifm[rot_hx(K, m)];
+        vr[m] = ur * g;
+        vi[m] = ui * g;
+    });
+    T sr[N], si[N];
+    swap_matvec<T, N, rot_moff(K) + 2 * N * N>(vr, vi, sr, si);
+    Unroll<0, T, N>::run([&](auto rc) {  // q = conj(phb) * s
+        constexpr int r = decltype(rc)::value;
+        const Z pb = ph_.B(r);
+        const T a = sr[r], b = si[r];
+        vr[r] = a * pb.re + b * pb.im;
+        vi[r] = b * pb.re - a * pb.im;
+    });
+    swap_matvec<T, N, rot_moff(K) + 2 * N * N>(vr, vi, sr, si);
+    Unroll<0, T, N>::run([&](auto rc) {  // out = i^r fm * pha * t
+        constexpr int r = decltype(rc)::value;
+        T orr = sr[r], oii = si[r];
+        mul_i_pow<r>(orr, oii);
+        const T f = c_fm[rot_hx(K, r)];
+        orr *= f;
+        oii *= f;
+        const Z pa = ph_.A(r);
+        col[ROTW_LD * rot_hx(K, r)] = mk<T>(orr * pa.re - oii * pa.im, orr * pa.im + oii * pa.re);
+    });
+    asm volatile("" ::: "memory");
+}
+
+template <typename T, int P, class PH, int... Ks>
+__device__ __forceinline__ void fwd_all(cplx<T>* col, const PH& ph_, std::integer_sequence<int, Ks...>) {
+    (fwd_degree<T, P, Ks, PH>(col, ph_), ...);
 }
 
 template <typename T, int P, class PH>
 __device__ __forceinline__ void rotw_fwd(cplx<T>* col, const PH& ph_) {
-    typedef cplx<T> Z;
-    // ---- 3) forward rotation and scatter into the column
-#pragma unroll
-    for (int n = 0; n <= P; ++n) {
-        T vr[P + 1], vi[P + 1];
-#pragma unroll
-        for (int m = 0; m <= n; ++m) {
-            const Z F = col[ROTW_LD * rot_hx(n, m)];
-            T ur, ui;  // (-i)^m F / fm
-            switch (m & 3) {
-                case 0: ur = F.re; ui = F.im; break;
-                case 1: ur = F.im; ui = -F.re; break;
-                case 2: ur = -F.re; ui = -F.im; break;
-                default: ur = -F.im; ui = F.re; break;
-            }
-            const T g = c_ifm[rot_hx(n, m)];
-            vr[m] = ur * g;
-            vi[m] = ui * g;
-        }
-        const T* Pt = c_rot + rot_moff(n) + 2 * (n + 1) * (n + 1);
-        const T* Qt = Pt + (n + 1) * (n + 1);
-        T sr[P + 1], si[P + 1];
-#pragma unroll
-        for (int r = 0; r <= n; ++r) {
-            T a = T(0), b = T(0);
-#pragma unroll
-            for (int q = 0; q <= n; ++q) a += Pt[r * (n + 1) + q] * vr[q];
-#pragma unroll
-            for (int q = 1; q <= n; ++q) b += Qt[r * (n + 1) + q] * vi[q];
-            const Z pb = ph_.B(r);  // conj(phb) * s
-            sr[r] = a * pb.re + b * pb.im;
-            si[r] = b * pb.re - a * pb.im;
-        }
-#pragma unroll
-        for (int r = 0; r <= n; ++r) {
-            T a = T(0), b = T(0);
-#pragma unroll
-            for (int q = 0; q <= n; ++q) a += Pt[r * (n + 1) + q] * sr[q];
-#pragma unroll
-            for (int q = 1; q <= n; ++q) b += Qt[r * (n + 1) + q] * si[q];
-            T orr, oii;  // i^r fm * t
-            switch (r & 3) {
-                case 0: orr = a; oii = b; break;
-                case 1: orr = -b; oii = a; break;
-                case 2: orr = -a; oii = -b; break;
-                default: orr = b; oii = -a; break;
-            }
-            const T f = c_fm[rot_hx(n, r)];
-            orr *= f;
-            oii *= f;
-            const Z pa = ph_.A(r);
-            col[ROTW_LD * rot_hx(n, r)] = mk<T>(orr * pa.re - oii * pa.im, orr * pa.im + oii * pa.re);
-        }
-        asm volatile("" ::: "memory");
-    }
+    fwd_all<T, P, PH>(col, ph_, std::make_integer_sequence<int, P + 1>{});
 }
 
 // FP64: the three phases are separate non-inlined functions so that each is
