@@ -115,6 +115,9 @@ SIGNATURES = {
     "fmmx_build_device": (_st, [_vp, _sz, _vp, _vp]),
     "fmmx_evaluate_device": (_st, [_vp, _vp, _vp, _vp, _vp]),
     "fmmx_synchronize": (_st, [_vp]),
+    "fmmx_leapfrog_device": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, C.c_int, C.c_int]),
+    "fmmx_build_ensemble": (_st, [_vp, _sz, _u64p, _dp, _dp]),
+    "fmmx_build_ensemble_device": (_st, [_vp, _sz, _u64p, _vp, _vp]),
     "fmmx_get_stats": (_st, [_vp, C.POINTER(Stats)]),
     "fmmx_export_tree": (_st, [_vp, _u32p, _u64p, _u32p, _i32p, _dp, _dp, _dp]),
     "fmmx_export_lists": (_st, [_vp, _u32p, _u32p]),
@@ -241,6 +244,20 @@ class Fmm:
         self.n = n
         self._check(lib().fmmx_build(self._h, n, _ptr(pos), _ptr(mass)))
 
+    def build_ensemble(self, offsets, mass, pos):
+        """Forest of independent systems: system s is bodies offsets[s]:offsets[s+1]."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        mass = _f64(mass)
+        pos = _f64(pos)
+        self._mass, self._pos = mass, pos
+        self.n = int(off[-1])
+        self._check(lib().fmmx_build_ensemble(self._h, len(off) - 1, _ptr(off, _u64p), _ptr(pos), _ptr(mass)))
+
+    def build_ensemble_device(self, offsets, pos_ptr: int, mass_ptr: int):
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self.n = int(off[-1])
+        self._check(lib().fmmx_build_ensemble_device(self._h, len(off) - 1, _ptr(off, _u64p), pos_ptr, mass_ptr))
+
     def run(self, mass=None, pos=None) -> Result:
         """Fmm::run: one force evaluation (bodies of the last build when None)."""
         n = self.n
@@ -266,6 +283,13 @@ class Fmm:
 
     def evaluate_device(self, pos_ptr, mass_ptr, acc_ptr, pot_ptr):
         self._check(lib().fmmx_evaluate_device(self._h, pos_ptr, mass_ptr, acc_ptr, pot_ptr))
+
+    def leapfrog_device(self, pos_ptr, vel_ptr, mass_ptr, acc_ptr, pot_ptr, dt, nsteps, scheme="kdk",
+                        refresh_every=1):
+        """Device-resident leapfrog; KDK needs acc at pos on entry."""
+        sc = {"kdk": 0, "dkd": 1}[scheme]
+        self._check(lib().fmmx_leapfrog_device(self._h, pos_ptr, vel_ptr, mass_ptr, acc_ptr, pot_ptr, float(dt),
+                                               int(nsteps), sc, int(refresh_every)))
 
     def synchronize(self):
         self._check(lib().fmmx_synchronize(self._h))

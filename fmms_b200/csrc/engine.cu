@@ -77,11 +77,16 @@ struct fmmx_ctx {
     std::vector<double> swap_host;
     DBuf<double> swap_dev;
 
-    // sizes of the current tree
+    // sizes of the current tree; a forest of nsys independent systems
     size_t n = 0;
+    int nsys = 1;
+    DBuf<uint64_t> sys_off;  // nsys + 1 offsets into the inputs
+    std::vector<uint64_t> sys_off_host;
+    int steps_since_build = 0;
+    DBuf<double> c_h;        // box size of every cell
     int nc = 0, nleaves = 0, nlevels = 0;
     int lvl_start[FMMX_NLEVELS + 1] = {0}, lvl_count[FMMX_NLEVELS + 1] = {0};
-    bool built = false, evaluated = false;
+    bool built = false, evaluated = false, lists_valid = false;
     int n_m2l = 0, n_p2p = 0;
     unsigned long long pops = 0, p2p_inter = 0;
 
@@ -298,13 +303,24 @@ M2lChoice m2l_choice(const fmmx_config& c) {
 const unsigned kGrid = 148u * 8u;
 
 // ---------------------------------------------------------------- build
-fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const double* d_mass) {
+// nsys > 1 builds a forest: system s is inputs [off[s], off[s+1]) (host
+// offsets), each with its own bounding box, keys, key sort and root.
+fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const double* d_mass, int nsys = 1,
+                       const uint64_t* h_off = nullptr) {
     cudaStream_t s = ctx->stream;
     if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input (the reference asserts !parts.is_empty(), tree.rs:95)");
     if (n >= (1ull << 31)) return fail(ctx, FMMX_INVALID_ARG, "n must be below 2^31");
+    if (nsys < 1) return fail(ctx, FMMX_INVALID_ARG, "no systems");
+    if (nsys > 1) {
+        if (h_off[0] != 0 || h_off[nsys] != n) return fail(ctx, FMMX_INVALID_ARG, "offsets must run from 0 to n");
+        for (int q = 0; q < nsys; ++q)
+            if (h_off[q + 1] <= h_off[q]) return fail(ctx, FMMX_INVALID_ARG, "every system needs at least one body");
+    }
     ctx->built = false;
     ctx->evaluated = false;
+    ctx->lists_valid = false;
     ctx->n = n;
+    ctx->nsys = nsys;
     if (ctx->events) CK(cudaEventRecord(ctx->ev[0], s), "event");
     CK(ctx->keys.ensure(n), "alloc keys");
     CK(ctx->keys_sorted.ensure(n), "alloc keys");
@@ -312,31 +328,50 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
     CK(ctx->order.ensure(n), "alloc order");
     for (DBuf<double>* b : {&ctx->x, &ctx->y, &ctx->z, &ctx->m, &ctx->nax, &ctx->nay, &ctx->naz, &ctx->npot})
         CK(b->ensure(n), "alloc bodies");
-    CK(ctx->box.ensure(8), "alloc box");
+    CK(ctx->box.ensure(8 * (size_t)nsys), "alloc box");
+    ctx->steps_since_build = 0;
+    if (nsys > 1) {
+        ctx->sys_off_host.assign(h_off, h_off + nsys + 1);
+        CK(ctx->sys_off.ensure(nsys + 1), "alloc offsets");
+        CK(cudaMemcpyAsync(ctx->sys_off.p, h_off, (nsys + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s), "copy");
+    }
     const unsigned gb = std::min<unsigned>(grid_for(n, 256), 1024u);
     CK(ctx->bbox_part.ensure(gb * 6), "alloc box");
     CK(ctx->flags.ensure(8), "alloc flags");
     CK(cudaMemsetAsync(ctx->flags.p, 0, 8 * sizeof(int), s), "memset");
 
     ctx->launches = 0;
-    k_bbox_partial<<<gb, 256, 0, s>>>(d_pos, n, ctx->bbox_part.p, ctx->flags.p + 2);
-    LCOUNT(5);  // bbox (2), keys, key sort (onesweep passes counted as 1), gather
-    k_bbox_final<<<1, 32, 0, s>>>(ctx->bbox_part.p, (int)gb, ctx->box.p);
-    k_keys<<<grid_for(n, 256), 256, 0, s>>>(d_pos, n, ctx->box.p, ctx->keys.p, ctx->idx.p);
-    CKL("keys");
     const int nbits = 3 * FMMX_BITS;
-    size_t tb = sort_pairs_u64_u32_temp((int)n, nbits);
-    CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-    CK(sort_pairs_u64_u32(ctx->cub_tmp.p, tb, ctx->keys.p, ctx->keys_sorted.p, ctx->idx.p, ctx->order.p, (int)n, nbits,
-                          s),
-       "key sort");
+    size_t tb;
+    LCOUNT(5);  // bbox (2), keys, key sort (onesweep passes counted as 1), gather
+    if (nsys == 1) {
+        k_bbox_partial<<<gb, 256, 0, s>>>(d_pos, n, ctx->bbox_part.p, ctx->flags.p + 2);
+        k_bbox_final<<<1, 32, 0, s>>>(ctx->bbox_part.p, (int)gb, ctx->box.p);
+        k_keys<<<grid_for(n, 256), 256, 0, s>>>(d_pos, n, ctx->box.p, ctx->keys.p, ctx->idx.p);
+        CKL("keys");
+        tb = sort_pairs_u64_u32_temp((int)n, nbits);
+        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+        CK(sort_pairs_u64_u32(ctx->cub_tmp.p, tb, ctx->keys.p, ctx->keys_sorted.p, ctx->idx.p, ctx->order.p, (int)n,
+                              nbits, s),
+           "key sort");
+    } else {
+        k_bbox_seg<<<nsys, 256, 0, s>>>(d_pos, ctx->sys_off.p, ctx->box.p, ctx->flags.p + 2);
+        k_keys_seg<<<grid_for(n, 256), 256, 0, s>>>(d_pos, n, ctx->sys_off.p, nsys, ctx->box.p, ctx->keys.p,
+                                                    ctx->idx.p);
+        CKL("keys");
+        tb = sort_pairs_seg_temp((int)n, nsys, ctx->sys_off.p, nbits);
+        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+        CK(sort_pairs_seg(ctx->cub_tmp.p, tb, ctx->keys.p, ctx->keys_sorted.p, ctx->idx.p, ctx->order.p, (int)n, nsys,
+                          ctx->sys_off.p, nbits, s),
+           "key sort");
+    }
     k_gather<<<grid_for(n, 256), 256, 0, s>>>(d_pos, d_mass, ctx->order.p, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p);
     CKL("gather");
 
     // level-by-level node creation, retried with more room on overflow
     CK(ctx->lvl.ensure(LV_SIZE), "alloc lvl");
-    if (ctx->tcap == 0) {
-        uint64_t est = 4ull * n / (uint64_t)std::max(ctx->cfg.n_leaf, 1) + 8ull * FMMX_NLEVELS + 64;
+    if (ctx->tcap == 0 || ctx->tcap < (uint32_t)nsys) {
+        uint64_t est = 4ull * n / (uint64_t)std::max(ctx->cfg.n_leaf, 1) + 8ull * FMMX_NLEVELS * nsys + 64;
         ctx->tcap = (uint32_t)std::min<uint64_t>(est, 0x7fffffffull);
     }
     int hl[LV_SIZE];
@@ -352,7 +387,8 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
         TmpNodes tn{ctx->t_first.p, ctx->t_count.p, ctx->t_parent.p, ctx->t_oct.p, ctx->t_level.p, ctx->t_leaf.p};
         CK(cudaMemsetAsync(ctx->lvl.p, 0, LV_SIZE * sizeof(int), s), "memset");
         CK(cudaMemsetAsync(ctx->flags.p, 0, 2 * sizeof(int), s), "memset");
-        k_tree_init<<<1, 32, 0, s>>>(tn, (uint32_t)n, ctx->lvl.p);
+        if (nsys == 1) k_tree_init<<<1, 32, 0, s>>>(tn, (uint32_t)n, ctx->lvl.p);
+        else k_tree_init_forest<<<grid_for(nsys, 128), 128, 0, s>>>(tn, ctx->sys_off.p, nsys, ctx->lvl.p);
         LCOUNT(1 + FMMX_NLEVELS);
         const unsigned gl = std::min<unsigned>(grid_for(cap, 256), kGrid);
         for (int L = 0; L < FMMX_NLEVELS; ++L)
@@ -418,6 +454,14 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
                                                             ctx->cfg.center_mode);
     }
     CKL("geometry");
+    CK(ctx->c_h.ensure(nc), "alloc cells");
+    for (int L = 0; L < nlev; ++L) {
+        const int cnt = ctx->lvl_count[L];
+        k_cell_h<<<grid_for(cnt, 256), 256, 0, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, ctx->c_parent.p,
+                                                    ctx->box.p, ctx->c_h.p);
+    }
+    LCOUNT(nlev);
+    CKL("cell sizes");
     if (ctx->events) CK(cudaEventRecord(ctx->ev[1], s), "event");
     CK(cudaStreamSynchronize(s), "build");
     if (ctx->events) {
@@ -466,9 +510,11 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
         w.cap_p2p = ctx->cap_p2p;
         CK(cudaMemsetAsync(ctx->wcounts.p, 0, WC_SIZE * sizeof(int), s), "memset");
         CK(cudaMemsetAsync(ctx->wpops.p, 0, sizeof(unsigned long long), s), "memset");
-        CK(cudaMemsetAsync(ctx->front0.p, 0, sizeof(uint2), s), "memset");  // root pair (0, 0)
-        const int one = 1;
-        CK(cudaMemcpyAsync(ctx->wcounts.p + WC_FRONT0, &one, sizeof(int), cudaMemcpyHostToDevice, s), "copy");
+        // seeds: the self pair of every root (one per system)
+        k_walk_init<<<grid_for(ctx->nsys, 128), 128, 0, s>>>(ctx->level_cells.p, ctx->nsys, ctx->front0.p);
+        LCOUNT(1);
+        const int seeds = ctx->nsys;  // pageable source: staged before the call returns
+        CK(cudaMemcpyAsync(ctx->wcounts.p + WC_FRONT0, &seeds, sizeof(int), cudaMemcpyHostToDevice, s), "copy");
         int cur = 0;
         int hc[WC_SIZE];
         bool done = false;
@@ -592,7 +638,12 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     return FMMX_OK;
 }
 
-fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+// reuse: keep the interaction lists of the last evaluation of this tree (no
+// f pre-pass, walk or list build); moments and locals are recomputed from the
+// given positions about the cell centres of the last build. This is the
+// tree reuse of the reference's GPU backend (crates/visual/src/gpufmm.rs:9-20).
+fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot,
+                          bool reuse = false) {
     cudaStream_t s = ctx->stream;
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
     const int p = ctx->cfg.p, dim = dimp(p), nc = ctx->nc;
@@ -611,7 +662,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     CK(ctx->pows.ensure((size_t)nc * (p + 1)), "alloc expansions");
     CK(ctx->fmin.ensure(nc), "alloc expansions");
     CK(ctx->f.ensure(n), "alloc expansions");
-    const bool dehnen = ctx->cfg.mac_mode == FMMX_MAC_DEHNEN;
+    if (reuse && !ctx->lists_valid) reuse = false;
+    const bool dehnen = ctx->cfg.mac_mode == FMMX_MAC_DEHNEN && !reuse;  // f pre-pass and power needed
     const bool mixed = ctx->cfg.precision == FMMX_MIXED;
     const int H = (p + 1) * (p + 2) / 2;
     const CellsView cv = view(ctx);
@@ -620,14 +672,13 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CK(ctx->loc_f.ensure((size_t)nc * H), "alloc expansions");
         CK(ctx->ell.ensure(nc), "alloc expansions");
         CK(ctx->ellf.ensure(nc), "alloc expansions");
-        k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_level.p, ctx->box.p, ctx->ell.p,
-                                                       ctx->ellf.p);
+        k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_h.p, ctx->ell.p, ctx->ellf.p);
         LCOUNT(1);
     }
     if (dehnen) {
         CK(cudaMemsetAsync(ctx->flags.p + 3, 0, sizeof(int), s), "memset");
-        k_fprepass<<<grid_for(n, 128), 128, 0, s>>>(cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, n, ctx->f.p,
-                                                    ctx->flags.p + 3);
+        k_fprepass<<<grid_for(n, 128), 128, 0, s>>>(cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, n, ctx->sys_off.p,
+                                                    ctx->nsys, ctx->level_cells.p, ctx->f.p, ctx->flags.p + 3);
         CKL("f pre-pass");
     }
     if (mixed && !dehnen) {
@@ -661,16 +712,21 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         }
     }
     if (tm) CK(cudaEventRecord(ev[3], s), "event");
-    fmmx_status st = walk_impl(ctx);
-    if (st != FMMX_OK) return st;
-    if (dehnen) {
-        int bad = 0;
-        CK(cudaMemcpy(&bad, ctx->flags.p + 3, sizeof(int), cudaMemcpyDeviceToHost), "copy");
-        if (bad) return fail(ctx, FMMX_DEVICE_ERROR, "f pre-pass stack overflow");
+    if (!reuse) {
+        fmmx_status st = walk_impl(ctx);
+        if (st != FMMX_OK) return st;
+        if (dehnen) {
+            int bad = 0;
+            CK(cudaMemcpy(&bad, ctx->flags.p + 3, sizeof(int), cudaMemcpyDeviceToHost), "copy");
+            if (bad) return fail(ctx, FMMX_DEVICE_ERROR, "f pre-pass stack overflow");
+        }
     }
     if (tm) CK(cudaEventRecord(ev[4], s), "event");
-    st = lists_impl(ctx);
-    if (st != FMMX_OK) return st;
+    if (!reuse) {
+        fmmx_status st = lists_impl(ctx);
+        if (st != FMMX_OK) return st;
+        ctx->lists_valid = true;
+    }
     if (tm) CK(cudaEventRecord(ev[5], s), "event");
 
     DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p};
@@ -872,6 +928,30 @@ fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double*
     return build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p);
 }
 
+fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* d_pos,
+                                       const double* d_mass) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!d_pos || !d_mass || !offsets || nsys == 0 || nsys > (1u << 24)) return fail(ctx, FMMX_INVALID_ARG, "bad input");
+    cudaSetDevice(ctx->cfg.device);
+    return build_impl(ctx, (size_t)offsets[nsys], d_pos, d_mass, (int)nsys, offsets);
+}
+
+fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* pos,
+                                const double* mass) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!pos || !mass || !offsets || nsys == 0 || nsys > (1u << 24)) return fail(ctx, FMMX_INVALID_ARG, "bad input");
+    const size_t n = (size_t)offsets[nsys];
+    if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input");
+    cudaSetDevice(ctx->cfg.device);
+    if (ctx->pos_in.ensure(3 * n) != cudaSuccess || ctx->mass_in.ensure(n) != cudaSuccess)
+        return fail(ctx, FMMX_OUT_OF_MEMORY, "input buffers");
+    cudaStream_t s = ctx->stream;
+    if (cudaMemcpyAsync(ctx->pos_in.p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->mass_in.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
+    return build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p, (int)nsys, offsets);
+}
+
 fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc,
                                  double* d_pot) {
     if (!ctx) return FMMX_INVALID_ARG;
@@ -882,6 +962,57 @@ fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const doubl
         d_pot = ctx->pot_out.p;
     }
     return evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot);
+}
+
+fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, const double* d_mass, double* d_acc,
+                                 double* d_pot, double dt, int nsteps, int scheme, int refresh_every) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    if (!d_pos || !d_vel || !d_mass || !d_acc || nsteps < 0 || refresh_every < 1 || (scheme != 0 && scheme != 1))
+        return fail(ctx, FMMX_INVALID_ARG, "bad leapfrog arguments");
+    if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "leapfrog needs a built tree (build + evaluate first)");
+    cudaSetDevice(ctx->cfg.device);
+    cudaStream_t s = ctx->stream;
+    const size_t n = ctx->n;
+    if (!d_pot) {
+        if (ctx->pot_out.ensure(n) != cudaSuccess) return fail(ctx, FMMX_OUT_OF_MEMORY, "pot buffer");
+        d_pot = ctx->pot_out.p;
+    }
+    const unsigned g = grid_for(3 * n, 256);
+    for (int step = 0; step < nsteps; ++step) {
+        const bool rebuild = (ctx->steps_since_build + 1) >= refresh_every;
+        if (scheme == 0) {  // kick-drift-kick; d_acc holds the forces at d_pos
+            k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
+            k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, dt);
+        } else {  // drift-kick-drift (crates/fmm/tests/energy_gate.rs:156-177)
+            k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, 0.5 * dt);
+        }
+        if (cudaGetLastError() != cudaSuccess) return fail(ctx, FMMX_DEVICE_ERROR, "leapfrog update");
+        fmmx_status st;
+        if (rebuild) {
+            if (ctx->nsys == 1) {
+                st = build_impl(ctx, n, d_pos, d_mass);
+            } else {
+                std::vector<uint64_t> off(ctx->sys_off_host);
+                st = build_impl(ctx, n, d_pos, d_mass, ctx->nsys, off.data());
+            }
+            if (st != FMMX_OK) return st;
+            ctx->steps_since_build = 0;
+            st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, false);
+        } else {
+            ctx->steps_since_build++;
+            st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, true);
+        }
+        if (st != FMMX_OK) return st;
+        if (scheme == 0) {
+            k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
+        } else {
+            k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, dt);
+            k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, 0.5 * dt);
+        }
+        if (cudaGetLastError() != cudaSuccess) return fail(ctx, FMMX_DEVICE_ERROR, "leapfrog update");
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "leapfrog");
+    return FMMX_OK;
 }
 
 fmmx_status fmmx_evaluate(fmmx_ctx* ctx, const double* pos, const double* mass, double* acc, double* pot) {

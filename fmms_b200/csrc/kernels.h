@@ -67,6 +67,13 @@ __global__ void k_keys(const double* pos, size_t n, const double* box, uint64_t*
 __global__ void k_gather(const double* pos, const double* mass, const uint32_t* order, size_t n, double* x,
                          double* y, double* z, double* m);
 __global__ void k_tree_init(TmpNodes t, uint32_t n, int* lvl);
+__global__ void k_bbox_seg(const double* pos, const uint64_t* off, double* box, int* bad);
+__global__ void k_keys_seg(const double* pos, size_t n, const uint64_t* off, int nsys, const double* box,
+                           uint64_t* keys, uint32_t* idx);
+__global__ void k_tree_init_forest(TmpNodes t, const uint64_t* off, int nsys, int* lvl);
+__global__ void k_cell_h(const int32_t* level_cells, int lstart, int lcnt, const int32_t* parent, const double* box,
+                         double* h);
+__global__ void k_walk_init(const int32_t* level_cells, int nroots, uint2* front);
 __global__ void k_build_level(TmpNodes t, const uint64_t* keys, int L, long long n_leaf, uint32_t cap, int* lvl,
                               int* flags);
 __global__ void k_dfs_keys(TmpNodes t, int nc, uint64_t* key, uint32_t* val);
@@ -80,7 +87,7 @@ __global__ void k_upward_exact(const int32_t* level_cells, int lstart, int lcnt,
                                const double* y, const double* z, const double* m, int p, zd* moments, double* pows,
                                const double* f, double* fmin);
 __global__ void k_fprepass(CellsView cells, const double* x, const double* y, const double* z, const double* m,
-                           size_t n, double* f, int* err);
+                           size_t n, const uint64_t* off, int nsys, const int32_t* roots, double* f, int* err);
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
 
 // lists.cu
@@ -106,8 +113,7 @@ __global__ void k_l2p_f64(size_t n, const int32_t* body_leaf, const uint32_t* or
 
 // mixed.cu
 void upload_tables_mixed(const OrderTables& t, cudaStream_t s);
-__global__ void k_cell_scale(int nc, const double* rho, const uint8_t* level, const double* box, double* ell,
-                             float* ellf);
+__global__ void k_cell_scale(int nc, const double* rho, const double* h, double* ell, float* ellf);
 __global__ void k_moments_to_mixed(int nc, int p, const zd* full, const double* ell, zf* half);
 void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
                          int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,
@@ -124,6 +130,10 @@ __global__ void k_p2p_mixed(DirList L, int ncells, CellsView cv, const double* x
 // p2p.cu
 __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,
                           const double* m, double soft2, double* ax, double* ay, double* az, double* pot);
+
+// integrate.cu
+__global__ void k_kick(size_t n3, double* v, const double* a, double h);
+__global__ void k_drift(size_t n3, double* x, const double* v, double h);
 
 // direct.cu
 __global__ void k_direct_targets(const double* pos, const double* mass, size_t n, const uint32_t* tgt, size_t nt,

@@ -119,7 +119,7 @@ struct Unroll {  // compile-time loop helper: f(integral_constant<m>) for m = M.
 
 template <typename T, int P, int K, bool FULL_LAYOUT, class PH>
 __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,
-                                            T& sak) {
+                                            T& sak, T cap) {
     typedef cplx<T> Z;
     constexpr int N = K + 1;
     T vr[N], vi[N];
@@ -151,26 +151,29 @@ __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, cons
         const T g = c_ifm[rot_hx(K, r)] * sak;
         col[ROTW_LD * rot_hx(K, r)] = mk<T>(orr * g, oii * g);
     });
-    sak *= sa;
+    sak = min(sak * sa, cap);
     asm volatile("" ::: "memory");  // keep degrees apart: bounds the live registers
 }
 
 template <typename T, int P, bool FULL_LAYOUT, class PH, int... Ks>
-__device__ __forceinline__ void back_all(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,
+__device__ __forceinline__ void back_all(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa, T cap,
                                          std::integer_sequence<int, Ks...>) {
     T sak = T(1);
-    (back_degree<T, P, Ks, FULL_LAYOUT, PH>(ms, ph_, col, sa, sak), ...);
+    (back_degree<T, P, Ks, FULL_LAYOUT, PH>(ms, ph_, col, sa, sak, cap), ...);
 }
 
+// `cap` bounds the scale powers of the normalised (mixed) form: a power only
+// exceeds 1 where the moments it multiplies are exactly zero (a cell of radius
+// 0), and the cap keeps that product 0 instead of 0 * inf.
 template <typename T, int P, bool FULL_LAYOUT, class PH>
-__device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa) {
-    back_all<T, P, FULL_LAYOUT, PH>(ms, ph_, col, sa, std::make_integer_sequence<int, P + 1>{});
+__device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa, T cap) {
+    back_all<T, P, FULL_LAYOUT, PH>(ms, ph_, col, sa, cap, std::make_integer_sequence<int, P + 1>{});
 }
 
 // axial translation of column m, in place:
 // F~[n][m] = (-1)^m conj(sum_{k=m}^{P-n} b[k][m] (n+k)!) sb^{n+1}
 template <typename T, int P, int M>
-__device__ __forceinline__ void axial_col(cplx<T>* col, T sb) {
+__device__ __forceinline__ void axial_col(cplx<T>* col, T sb, T cap) {
     constexpr int L = P - M + 1;  // entries k = M..P
     T br[L], bi[L];
     Unroll<0, T, L>::run([&](auto jc) {
@@ -181,7 +184,7 @@ __device__ __forceinline__ void axial_col(cplx<T>* col, T sb) {
     });
     T sbn = sb;
 #pragma unroll
-    for (int n = 0; n < M; ++n) sbn *= sb;
+    for (int n = 0; n < M; ++n) sbn = min(sbn * sb, cap);
     constexpr T sg = (M & 1) ? T(-1) : T(1);
     Unroll<M, T, P + 1>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
@@ -192,19 +195,19 @@ __device__ __forceinline__ void axial_col(cplx<T>* col, T sb) {
             ai += bi[k - M] * c_fact[n + k];
         });
         col[ROTW_LD * rot_hx(n, M)] = mk<T>(sg * ar * sbn, -sg * ai * sbn);
-        sbn *= sb;
+        sbn = min(sbn * sb, cap);
     });
     asm volatile("" ::: "memory");
 }
 
 template <typename T, int P, int... Ms>
-__device__ __forceinline__ void axial_all(cplx<T>* col, T sb, std::integer_sequence<int, Ms...>) {
-    (axial_col<T, P, Ms>(col, sb), ...);
+__device__ __forceinline__ void axial_all(cplx<T>* col, T sb, T cap, std::integer_sequence<int, Ms...>) {
+    (axial_col<T, P, Ms>(col, sb, cap), ...);
 }
 
 template <typename T, int P>
-__device__ __forceinline__ void rotw_axial(cplx<T>* col, T sb) {
-    axial_all<T, P>(col, sb, std::make_integer_sequence<int, P + 1>{});
+__device__ __forceinline__ void rotw_axial(cplx<T>* col, T sb, T cap) {
+    axial_all<T, P>(col, sb, cap, std::make_integer_sequence<int, P + 1>{});
 }
 
 template <typename T, int P, int K, class PH>
@@ -259,12 +262,12 @@ __device__ __forceinline__ void rotw_fwd(cplx<T>* col, const PH& ph_) {
 // register file and spill).
 template <typename T, int P, bool FULL_LAYOUT>
 __device__ __noinline__ void rotw_back_ni(const cplx<T>* __restrict__ ms, const cplx<T>* pa, const cplx<T>* pb,
-                                          cplx<T>* col, T sa) {
-    rotw_back<T, P, FULL_LAYOUT>(ms, PhSmem<T>{pa, pb}, col, sa);
+                                          cplx<T>* col, T sa, T cap) {
+    rotw_back<T, P, FULL_LAYOUT>(ms, PhSmem<T>{pa, pb}, col, sa, cap);
 }
 template <typename T, int P>
-__device__ __noinline__ void rotw_axial_ni(cplx<T>* col, T sb) {
-    rotw_axial<T, P>(col, sb);
+__device__ __noinline__ void rotw_axial_ni(cplx<T>* col, T sb, T cap) {
+    rotw_axial<T, P>(col, sb, cap);
 }
 template <typename T, int P>
 __device__ __noinline__ void rotw_fwd_ni(cplx<T>* col, const cplx<T>* pa, const cplx<T>* pb) {
@@ -331,13 +334,14 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
                 sb = (T)iR;
             }
             const Z* ms = mom + (size_t)src * (FULL_LAYOUT ? DIM : H);
+            const T cap = SCALED ? T(1e30) : T(INFINITY);
             if constexpr (PH_REGS) {
-                rotw_back<T, P, FULL_LAYOUT>(ms, phr, col, sa);
-                rotw_axial<T, P>(col, sb);
+                rotw_back<T, P, FULL_LAYOUT>(ms, phr, col, sa, cap);
+                rotw_axial<T, P>(col, sb, cap);
                 rotw_fwd<T, P>(col, phr);
             } else {
-                rotw_back_ni<T, P, FULL_LAYOUT>(ms, pha, phb, col, sa);
-                rotw_axial_ni<T, P>(col, sb);
+                rotw_back_ni<T, P, FULL_LAYOUT>(ms, pha, phb, col, sa, cap);
+                rotw_axial_ni<T, P>(col, sb, cap);
                 rotw_fwd_ni<T, P>(col, pha, phb);
             }
         }

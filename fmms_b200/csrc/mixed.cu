@@ -58,13 +58,16 @@ __device__ __forceinline__ void ups_column(A x, A y, A z, A r2, int p, int m, cp
     }
 }
 
-// Normalising length of every cell: rho, or side 2^{-level-10} for rho = 0.
-__global__ void k_cell_scale(int nc, const double* __restrict__ rho, const uint8_t* __restrict__ level,
-                             const double* __restrict__ box, double* __restrict__ ell, float* __restrict__ ellf) {
-    const double side = box[6];
+// Normalising length of every cell: rho, or the cell's box size h when rho = 0
+// (a single body, or coincident bodies: then every moment above the monopole
+// is exactly zero and any positive length works), kept >= 1e-30 so that it is
+// a normal FP32 number (a system of coincident bodies has box size DBL_MIN).
+__global__ void k_cell_scale(int nc, const double* __restrict__ rho, const double* __restrict__ h,
+                             double* __restrict__ ell, float* __restrict__ ellf) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         double l = rho[c];
-        if (!(l > 0.0)) l = ldexp(side, -(int)level[c] - 10);
+        if (!(l > 0.0)) l = h[c];
+        l = fmax(l, 1e-30);
         ell[c] = l;
         ellf[c] = (float)l;
     }
@@ -310,12 +313,11 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
                 }
             }
         }
-        const double s1 = il, s2 = il * il;
         const uint32_t id = order[k];
-        acc[3 * (size_t)id + 0] = nax[k] - (double)p11r * s2;
-        acc[3 * (size_t)id + 1] = nay[k] - (double)p11i * s2;
-        acc[3 * (size_t)id + 2] = naz[k] - (double)p10 * s2;
-        pot[id] = npot[k] + (double)p00 * s1;
+        acc[3 * (size_t)id + 0] = nax[k] - ((double)p11r * il) * il;
+        acc[3 * (size_t)id + 1] = nay[k] - ((double)p11i * il) * il;
+        acc[3 * (size_t)id + 2] = naz[k] - ((double)p10 * il) * il;
+        pot[id] = npot[k] + (double)p00 * il;
     }
 }
 

@@ -77,6 +77,54 @@ __global__ void k_bbox_final(const double* __restrict__ part, int nparts, double
     box[7] = 1.0 / side;
 }
 
+// Forest of independent systems (segments [off[s], off[s+1]) of the input):
+// one block per system reduces its own box.
+__global__ void k_bbox_seg(const double* __restrict__ pos, const uint64_t* __restrict__ off,
+                           double* __restrict__ box, int* __restrict__ bad) {
+    const int sys = blockIdx.x;
+    const uint64_t b = off[sys], e = off[sys + 1];
+    double lo[3] = {INFINITY, INFINITY, INFINITY};
+    double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int nonfinite = 0;
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double v = pos[3 * i + d];
+            nonfinite |= !isfinite(v);
+            lo[d] = fmin(lo[d], v);
+            hi[d] = fmax(hi[d], v);
+        }
+    }
+    __shared__ double sh[6][256];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sh[d][threadIdx.x] = lo[d];
+        sh[3 + d][threadIdx.x] = hi[d];
+    }
+    if (nonfinite) atomicOr(bad, 1);
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                sh[d][threadIdx.x] = fmin(sh[d][threadIdx.x], sh[d][threadIdx.x + w]);
+                sh[3 + d][threadIdx.x] = fmax(sh[3 + d][threadIdx.x], sh[3 + d][threadIdx.x + w]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double* bx = box + 8 * sys;
+        for (int d = 0; d < 3; ++d) {
+            bx[d] = sh[d][0];
+            bx[3 + d] = sh[3 + d][0];
+        }
+        const double side = fmax(fmax(fmax(bx[3] - bx[0], bx[4] - bx[1]), bx[5] - bx[2]), DBL_MIN);
+        bx[6] = side;
+        bx[7] = 1.0 / side;
+    }
+}
+
 // ------------------------------------------------------------ Morton keys
 // dilate, tree.rs:28-35
 __device__ __forceinline__ uint64_t dilate21(uint64_t x) {
@@ -100,6 +148,25 @@ __global__ void k_keys(const double* __restrict__ pos, size_t n, const double* _
                        uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
     const double lo0 = box[0], inv = box[7];
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t k = dilate21(quant(pos[3 * i + 2], lo0, inv));
+        k |= dilate21(quant(pos[3 * i + 1], lo0, inv)) << 1;
+        k |= dilate21(quant(pos[3 * i + 0], lo0, inv)) << 2;
+        keys[i] = k;
+        idx[i] = (uint32_t)i;
+    }
+}
+
+// Keys of a forest: each body is quantised in its own system's box.
+__global__ void k_keys_seg(const double* __restrict__ pos, size_t n, const uint64_t* __restrict__ off, int nsys,
+                           const double* __restrict__ box, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nsys;  // last system with off[sys] <= i
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (off[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        const double lo0 = box[8 * lo], inv = box[8 * lo + 7];
         uint64_t k = dilate21(quant(pos[3 * i + 2], lo0, inv));
         k |= dilate21(quant(pos[3 * i + 1], lo0, inv)) << 1;
         k |= dilate21(quant(pos[3 * i + 0], lo0, inv)) << 2;
@@ -136,6 +203,40 @@ __global__ void k_tree_init(TmpNodes t, uint32_t n, int* __restrict__ lvl) {
         t.level[0] = 0;
         lvl[LV_START + 0] = 0;
         lvl[LV_COUNT + 0] = 1;
+    }
+}
+
+// One root per system.
+__global__ void k_tree_init_forest(TmpNodes t, const uint64_t* __restrict__ off, int nsys, int* __restrict__ lvl) {
+    for (int sys = blockIdx.x * blockDim.x + threadIdx.x; sys < nsys; sys += gridDim.x * blockDim.x) {
+        t.first[sys] = (uint32_t)off[sys];
+        t.count[sys] = (uint32_t)(off[sys + 1] - off[sys]);
+        t.parent[sys] = -1;
+        t.oct[sys] = 0;
+        t.level[sys] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        lvl[LV_START + 0] = 0;
+        lvl[LV_COUNT + 0] = nsys;
+    }
+}
+
+// Box size of every cell: a root gets its system's box side, a child half its
+// parent's. Level 0 lists the roots in system order.
+__global__ void k_cell_h(const int32_t* __restrict__ level_cells, int lstart, int lcnt, const int32_t* __restrict__ parent,
+                         const double* __restrict__ box, double* __restrict__ h) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < lcnt; j += gridDim.x * blockDim.x) {
+        const int c = level_cells[lstart + j];
+        const int par = parent[c];
+        h[c] = par < 0 ? box[8 * j + 6] : 0.5 * h[par];
+    }
+}
+
+// Walk seeds: the self pair of every root.
+__global__ void k_walk_init(const int32_t* __restrict__ level_cells, int nroots, uint2* __restrict__ front) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nroots; j += gridDim.x * blockDim.x) {
+        const int r = level_cells[j];
+        front[j] = make_uint2(r, r);
     }
 }
 
@@ -551,15 +652,28 @@ __global__ void k_upward_exact(const int32_t* __restrict__ level_cells, int lsta
 // ------------------------------------------------------------ f pre-pass
 // f_walk, mac.rs:99-147: monopole treecode estimate of f_b = sum m/r^2 with a
 // LIFO stack (children pushed in octant order, so popped in reverse).
+// In a forest the walk starts at the root of the body's own system (roots
+// are level 0, in system order; slots of system s are [off[s], off[s+1])).
 __global__ void k_fprepass(CellsView cells, const double* __restrict__ x, const double* __restrict__ y,
                            const double* __restrict__ z, const double* __restrict__ m, size_t n,
+                           const uint64_t* __restrict__ off, int nsys, const int32_t* __restrict__ roots,
                            double* __restrict__ f, int* __restrict__ err) {
     constexpr int STACK = 8 * FMMX_NLEVELS;
     int stack[STACK];
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const double px = x[i], py = y[i], pz = z[i];
+        int root = 0;
+        if (nsys > 1) {
+            int lo = 0, hi = nsys;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (off[mid] <= i) lo = mid;
+                else hi = mid;
+            }
+            root = roots[lo];
+        }
         int sp = 0;
-        stack[sp++] = 0;
+        stack[sp++] = root;
         double fi = 0.0;
         while (sp > 0) {
             const int c = stack[--sp];

@@ -123,6 +123,32 @@ fmmx_status fmmx_build_device(fmmx_ctx* ctx, size_t n, const double* d_pos_xyz, 
 fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos_xyz, const double* d_mass, double* d_acc_xyz,
                                  double* d_pot);
 
+/* Batched ensemble (no reference counterpart): build one forest over nsys
+ * independent systems held back to back in the inputs; system s is bodies
+ * [offsets[s], offsets[s+1]) (host array of nsys + 1 entries, offsets[0] = 0,
+ * every system non-empty). Each system gets its own bounding box, keys, sort
+ * and root, and no interaction crosses systems; one fmmx_evaluate then covers
+ * all of them in the same launches, and every system's result is the one it
+ * gets alone (same arithmetic in the same order). */
+fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* pos_xyz,
+                                const double* mass);
+fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* d_pos_xyz,
+                                       const double* d_mass);
+
+/* Device-resident leapfrog (the integration loop of
+ * crates/fmm/tests/energy_gate.rs:133-219, which drifts and kicks on the host
+ * around Fmm::refresh + run). scheme 0 is kick-drift-kick: on entry d_acc must
+ * hold the accelerations at d_pos (a build + evaluate, or a previous call);
+ * scheme 1 is the reference test's drift-kick-drift. Positions and
+ * velocities (n x 3) are updated in place, d_acc/d_pot (nullable) hold the
+ * last evaluation. The tree is rebuilt every `refresh_every` steps (1 = every
+ * step); in between, the tree and interaction lists are reused and only the
+ * moments and locals are recomputed (tree reuse, gpufmm.rs:9-20). Works on a
+ * forest too. No reference counterpart as a library call. */
+fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos_xyz, double* d_vel_xyz, const double* d_mass,
+                                 double* d_acc_xyz, double* d_pot, double dt, int nsteps, int scheme,
+                                 int refresh_every);
+
 /* Wait for the context's stream. */
 fmmx_status fmmx_synchronize(fmmx_ctx* ctx);
 
