@@ -40,6 +40,10 @@ CONFIGS = {
     "c3": dict(gen="clusters", n=1 << 22, p=12, theta=0.4, softening=1e-5, n_leaf=32,
                workload="64 Plummer clusters N=4194304, a log-uniform[1e-3,1e-1], softening 1e-5, p=12, theta=0.4, leaf 32"),
 }
+EXTRA_CONFIGS = {
+    "c4": dict(gen="ensemble", n=0, p=8, theta=0.5, softening=1e-3, n_leaf=64, workload="ensemble"),
+    "c5": dict(gen="serve", n=0, p=8, theta=0.5, softening=1e-3, n_leaf=64, workload="serving"),
+}
 SEEDS = {"plummer_ic": 11, "uniform": 22, "clusters": 33}
 METRIC = "bodies/s at p99 force err <=1e-5 (mixed vs FP64 plain, 1 B200); p50/p99 step ms"
 
@@ -95,13 +99,17 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 "-lms", "50", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            t0 = time.time()  # the timed region starts once the sampler is writing
+            while time.time() - t0 < 5 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(0.12)  # at least one sample after the last timed step
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -177,22 +185,21 @@ def run_reference(args, cfg, rank):
 
 
 # ------------------------------------------------------------------ GPU arm
-def run_gpu(args, cfg, rank, world, local_rank):
+def measure_eval(args, cfg, precision, mass, pos, dev, world, clk_sampler=None):
+    """Time one force evaluation (build + evaluate) per step on device-resident
+    inputs, then the same through the host API (e2e), then the accuracy."""
     import torch
 
     import fmms_b200 as fx
 
-    dev = local_rank
-    torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
-    mass, pos = make_inputs(fx, cfg)
     n = len(mass)
     d_pos = torch.from_numpy(pos).to(f"cuda:{dev}")
     d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
     d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
     d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
-    kw = dict(mac="theta", theta=cfg["theta"], softening=cfg["softening"], precision=args.precision, m2l=args.m2l,
+    kw = dict(mac="theta", theta=cfg["theta"], softening=cfg["softening"], precision=precision, m2l=args.m2l,
               device=dev, stream=stream.cuda_stream)
     g = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], **kw)
 
@@ -209,7 +216,8 @@ def run_gpu(args, cfg, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     times, m2l_ms, p2p_ms, st = [], [], [], None
-    with ClockSampler(dev) as clk:
+    ctx_clk = clk_sampler if clk_sampler is not None else _NullCtx()
+    with ctx_clk:
         for _ in range(args.steps):
             flush.zero_()  # L2 flush between timed steps (untimed)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -231,8 +239,6 @@ def run_gpu(args, cfg, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
         total_ms = float(t.item())
-    ms_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms * 1e-3)
 
     # end to end through the host API: pinned host inputs in, host results out
     h_pos = torch.from_numpy(pos).pin_memory()
@@ -260,23 +266,57 @@ def run_gpu(args, cfg, rank, world, local_rank):
     a_ref, _, _ = fx.direct_targets(mass, pos, tg, softening=cfg["softening"], device=dev)
     acc = h_acc.numpy()
     rel = np.linalg.norm(acc[tg] - a_ref, axis=1) / np.linalg.norm(a_ref, axis=1)
+    g.close()
+    return dict(times=times, total_ms=total_ms, m2l_ms=sum(m2l_ms) / len(m2l_ms), p2p_ms=sum(p2p_ms) / len(p2p_ms),
+                st=st, e2e_ms=e2e_ms, rel=rel, ntargets=len(tg))
 
-    if rank != 0:
-        return
-    # roofline of the dominant kernel (M2L), from its own CUDA events
+
+class _NullCtx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def roofline(args, cfg, r, precision, dev):
+    import fmms_b200 as fx
+
+    st = r["st"]
     kernel = "naive" if args.m2l == "naive" else "rotation"
     fl = st["m2l_directed"] * m2l_flops_per_translation(cfg["p"], kernel)
-    m2l_avg = sum(m2l_ms) / len(m2l_ms)
-    fp64 = args.precision == "plain"
+    fp64 = precision == "plain"
     peak = fx.probe_fma_peak(fp64=fp64, device=dev)
-    achieved = fl / (m2l_avg * 1e-3) / 1e12
-    roof = {"bound": "fp64" if fp64 else "fp32", "kernel": "m2l", "achieved": achieved, "peak": peak,
+    achieved = fl / (r["m2l_ms"] * 1e-3) / 1e12
+    return {"bound": "fp64" if fp64 else "fp32", "kernel": "m2l", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
             "peak_source": "measured: FMA loop on every SM (fmmx_probe_fma_peak); MEASURED_PEAKS.json holds only "
                            "HBM and bf16-tensor peaks",
-            "algorithmic_flops_per_launch": fl, "launch_ms": m2l_avg,
-            "p2p": {"achieved": p2p_flops(st["p2p_interactions"]) / (sum(p2p_ms) / len(p2p_ms) * 1e-3) / 1e12,
-                    "unit": "TFLOP/s", "ms": sum(p2p_ms) / len(p2p_ms)}}
+            "algorithmic_flops_per_launch": fl, "launch_ms": r["m2l_ms"],
+            "p2p": {"achieved": p2p_flops(st["p2p_interactions"]) / (r["p2p_ms"] * 1e-3) / 1e12,
+                    "unit": "TFLOP/s", "ms": r["p2p_ms"]}}
+
+
+def run_gpu(args, cfg, rank, world, local_rank):
+    import torch
+
+    import fmms_b200 as fx
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    mass, pos = make_inputs(fx, cfg)
+    n = len(mass)
+    clk = ClockSampler(dev)
+    main = measure_eval(args, cfg, args.precision, mass, pos, dev, world, clk)
+    other = None
+    if not args.no_compare:
+        other_prec = "plain" if args.precision == "mixed" else "mixed"
+        other = measure_eval(args, cfg, other_prec, mass, pos, dev, world)
+    if rank != 0:
+        return
+    value = world * n * args.steps / (main["total_ms"] * 1e-3)
+    st = main["st"]
+    rel = main["rel"]
     cpu = None
     if world == 1 and not args.no_cpu:
         nth = os.cpu_count() or 1
@@ -284,26 +324,229 @@ def run_gpu(args, cfg, rank, world, local_rank):
         cpu = {"value": bps, "unit": "bodies/s", "cores": nth, "kind": "port",
                "sample": f"{args.cpu_sample} bodies of the same generator and settings, one threaded evaluation "
                          f"of the oracle's restatement of the reference FMM ({dt:.1f} s)"}
-    clocks = clk.summary()
+    fp64 = args.precision == "plain"
     line = {
         "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": main["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
         "config": {"workload": cfg["workload"], "precision": args.precision, "n": n, "p": cfg["p"],
                    "theta": cfg["theta"], "n_leaf": cfg["n_leaf"], "l2": "flushed between timed steps",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "step_ms_p50": float(np.percentile(times, 50)), "step_ms_p99": float(np.percentile(times, 99)),
+        "step_ms_p50": float(np.percentile(main["times"], 50)),
+        "step_ms_p99": float(np.percentile(main["times"], 99)),
         "force_err": {"p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99)),
-                      "max": float(rel.max()), "targets": len(tg), "reference": "FP64 direct sum"},
-        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "bodies/s", "h2d_bytes_per_step": 32 * n,
-                "d2h_bytes_per_step": 32 * n, "ms_per_step": e2e_ms},
+                      "max": float(rel.max()), "targets": main["ntargets"], "reference": "FP64 direct sum"},
+        "e2e": {"value": world * n / (main["e2e_ms"] * 1e-3), "unit": "bodies/s", "h2d_bytes_per_step": 32 * n,
+                "d2h_bytes_per_step": 32 * n, "ms_per_step": main["e2e_ms"]},
         "gpu_launches": int(st["kernel_launches"]) * args.steps,
         "stages_ms": {k[3:]: round(v, 3) for k, v in st.items() if k.startswith("ms_")},
         "counts": {k: int(st[k]) for k in ("n_cells", "n_leaves", "n_m2l", "n_p2p", "p2p_interactions")},
-        "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+        "roofline": roofline(args, cfg, main, args.precision, dev), "cpu_baseline": cpu, "clocks": clk.summary(),
     }
+    if other is not None:
+        orel = other["rel"]
+        ov = world * n * args.steps / (other["total_ms"] * 1e-3)
+        line["compare"] = {"precision": "plain" if args.precision == "mixed" else "mixed", "value": ov,
+                           "ms_per_step": other["total_ms"] / args.steps,
+                           "force_err_p50": float(np.percentile(orel, 50)),
+                           "force_err_p99": float(np.percentile(orel, 99)),
+                           "stages_ms": {k[3:]: round(v, 3) for k, v in other["st"].items() if k.startswith("ms_")},
+                           "speedup_of_main": value / ov}
     print(json.dumps(line), flush=True)
-    g.close()
+
+
+# ------------------------------------------------------------------ C3: KDK
+def run_kdk(args, cfg, rank, world, local_rank):
+    """Clustered deep-tree workload: ten kick-drift-kick steps (dt = 1e-4),
+    mixed and plain, force error against the direct sum at every step."""
+    import torch
+
+    import fmms_b200 as fx
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    mass, pos, vel = fx.gen_clusters(cfg["n"], 64, 1e-3, 1e-1, SEEDS["clusters"])
+    n = len(mass)
+    rng = np.random.default_rng(4096)
+    tg = np.sort(rng.choice(n, size=4096, replace=False)).astype(np.uint32)
+    out = {}
+    for prec in ([args.precision] + ([] if args.no_compare else ["plain" if args.precision == "mixed" else "mixed"])):
+        d_pos = torch.from_numpy(pos.copy()).to(f"cuda:{dev}")
+        d_vel = torch.from_numpy(vel.copy()).to(f"cuda:{dev}")
+        d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
+        d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+        d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+        g = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], mac="theta", theta=cfg["theta"],
+                   softening=cfg["softening"], precision=prec, device=dev, stream=stream.cuda_stream)
+        g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+        g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+        step_ms, errs = [], []
+        for k in range(args.kdk_steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.leapfrog_device(d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
+                              d_pot.data_ptr(), 1e-4, 1, "kdk", args.refresh_every)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            p_now = d_pos.cpu().numpy()
+            a_ref, _, _ = fx.direct_targets(mass, p_now, tg, softening=cfg["softening"], device=dev)
+            a = d_acc.cpu().numpy()[tg]
+            rel = np.linalg.norm(a - a_ref, axis=1) / np.linalg.norm(a_ref, axis=1)
+            errs.append({"p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99))})
+        out[prec] = {"bodies_per_s": n * len(step_ms) / (sum(step_ms) * 1e-3), "step_ms": step_ms,
+                     "force_err_per_step": errs, "stages_ms_last": {k[3:]: round(v, 3) for k, v in g.stats().items()
+                                                                    if k.startswith("ms_")}}
+        g.close()
+    if rank != 0:
+        return
+    main = out[args.precision]
+    line = {"metric": METRIC, "value": main["bodies_per_s"], "unit": "bodies/s", "n_gpus": world,
+            "steps": args.kdk_steps, "warmup": 0, "ms_per_step": float(np.mean(main["step_ms"])),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "dtype": "f64" if args.precision == "plain" else "f32+f64",
+            "config": {"workload": cfg["workload"] + ", 10 KDK steps dt=1e-4", "refresh_every": args.refresh_every},
+            "step_ms_p50": float(np.percentile(main["step_ms"], 50)),
+            "step_ms_p99": float(np.percentile(main["step_ms"], 99)), "kdk": out}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ C4: ensemble
+def run_ensemble(args, cfg, rank, world, local_rank):
+    """512 independent Plummer spheres (N log-uniform in [1e3, 1e5], scale
+    radius U[0.5, 2], mass 1 each) in one forest; per-system error on 256
+    seeded targets each."""
+    import torch
+
+    import fmms_b200 as fx
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(512)
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(1e5), args.nsys)).astype(np.int64)
+    radii = rng.uniform(0.5, 2.0, args.nsys)
+    parts = [fx.gen_plummer_ic(int(nn), 1.0, float(a), 20.0, 1000 + i, velocities=False)[:2]
+             for i, (nn, a) in enumerate(zip(sizes, radii))]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    mass = np.concatenate([m for m, _ in parts])
+    pos = np.concatenate([p for _, p in parts])
+    n = len(mass)
+    tune = None
+    n_leaf, p_use, tile = cfg["n_leaf"], cfg["p"], 0
+    if args.autotune:
+        from fmms_b200.autotune import tune_ensemble
+
+        tune = tune_ensemble(parts, p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"],
+                             precision=args.precision, device=dev)
+        n_leaf, p_use, tile = tune["n_leaf"], tune["p"], tune["p2p_tile"]
+    d_pos = torch.from_numpy(pos).to(f"cuda:{dev}")
+    d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+    d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+    g = fx.Fmm(None, None, p_use, 0.0, n_leaf, mac="theta", theta=cfg["theta"], softening=cfg["softening"],
+               precision=args.precision, device=dev, stream=stream.cuda_stream, p2p_tile=tile)
+
+    def step():
+        g.build_ensemble_device(off, d_pos.data_ptr(), d_mass.data_ptr())
+        g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    acc = d_acc.cpu().numpy()
+    p99s = []
+    for i, (m, p) in enumerate(parts):
+        t = np.sort(np.random.default_rng(i).choice(len(m), size=min(256, len(m)), replace=False)).astype(np.uint32)
+        a_ref, _, _ = fx.direct_targets(m, p, t, softening=cfg["softening"], device=dev)
+        a = acc[int(off[i]):int(off[i + 1])][t]
+        rel = np.linalg.norm(a - a_ref, axis=1) / np.linalg.norm(a_ref, axis=1)
+        p99s.append(float(np.percentile(rel, 99)))
+    if rank != 0:
+        return
+    st = g.stats()
+    ms = float(np.mean(times))
+    line = {"metric": METRIC, "value": n / (ms * 1e-3), "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "dtype": "f64" if args.precision == "plain" else "f32+f64",
+            "config": {"workload": f"{args.nsys} Plummer systems, N log-uniform[1e3,1e5] (total {n}), one forest",
+                       "p": p_use, "n_leaf": n_leaf, "p2p_tile": tile,
+                       "autotune": {k: v for k, v in (tune or {}).items() if k != "candidates"}},
+            "per_system_force_err_p99": {"median": float(np.median(p99s)), "max": float(np.max(p99s))},
+            "stages_ms": {k[3:]: round(v, 3) for k, v in st.items() if k.startswith("ms_")},
+            "gpu_launches": int(st["kernel_launches"]) * args.steps}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ C5: serving
+def run_serve(args, cfg, rank, world, local_rank):
+    """Poisson arrivals (args.rate per second for args.duration seconds) of
+    Plummer or uniform-cube sessions (50/50), N log-uniform in [1e3, 1e6], 100
+    KDK steps of dt = 1e-3 each, admitted under the HBM budget."""
+    import fmms_b200 as fx
+    from fmms_b200.serve import Server, Session, run_session_alone
+
+    if rank != 0:
+        return
+    rng = np.random.default_rng(5)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=int(args.rate * args.duration * 2) + 10))
+    arrivals = arrivals[arrivals < args.duration]
+    sessions = []
+    for i, t in enumerate(arrivals):
+        nn = int(np.exp(rng.uniform(np.log(1e3), np.log(args.serve_nmax))))
+        if rng.random() < 0.5:
+            m, p, v = fx.gen_plummer_ic(nn, 1.0, 1.0, 20.0, 7000 + i)
+        else:
+            m, p = fx.gen_uniform_lognormal(nn, 0.5, 7000 + i)
+            v = np.zeros_like(p)
+        sessions.append(Session(sid=i, mass=m, pos=p, vel=v, steps=args.serve_steps, dt=1e-3, arrival=float(t)))
+    kw = dict(p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"], n_leaf=cfg["n_leaf"],
+              precision=args.precision, budget_bytes=args.budget_gb * 1e9, max_active_bodies=args.max_active)
+    srv = Server(**kw)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        now = time.perf_counter() - t0
+        while k < len(sessions) and sessions[k].arrival <= now:
+            srv.submit(sessions[k])
+            k += 1
+        if now > args.duration and not srv.active:
+            break
+        if now > args.duration + args.drain:
+            break
+        if not srv.active and not srv.queue:
+            time.sleep(0.001)
+            continue
+        srv.tick()
+    rep = srv.report()
+    # isolated step latency of a few completed sessions, to compare with the mix
+    ratios = []
+    for s in srv.done[: args.isolated_samples]:
+        _, _, alone_ms = run_session_alone(s, **{k2: v for k2, v in kw.items() if k2 != "max_active_bodies"})
+        ratios.append(float(np.percentile(s.step_ms, 99) / max(np.percentile(alone_ms, 50), 1e-6)))
+    line = {"metric": METRIC, "value": rep["bodies_per_s"], "unit": "bodies/s", "n_gpus": 1, "steps": rep["ticks"],
+            "warmup": 0, "ms_per_step": float(np.mean(srv.tick_ms)) if srv.tick_ms else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "dtype": "f64" if args.precision == "plain" else "f32+f64",
+            "config": {"workload": f"serving: Poisson {args.rate}/s for {args.duration}s, N log-uniform[1e3,"
+                                   f"{args.serve_nmax:.0e}], {args.serve_steps} KDK steps", "budget_gb": args.budget_gb},
+            "serve": {**rep, "arrived": len(sessions), "submitted": k, "queued_at_end": len(srv.queue),
+                      "active_at_end": len(srv.active),
+                      "p99_over_isolated": {"median": float(np.median(ratios)) if ratios else None,
+                                            "max": float(np.max(ratios)) if ratios else None,
+                                            "samples": len(ratios)}}}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -312,13 +555,26 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fmmx", choices=["fmmx", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4", "c5"])
+    ap.add_argument("--precision", default="mixed", choices=["plain", "mixed"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the other precision's run")
+    ap.add_argument("--kdk-steps", type=int, default=10)
+    ap.add_argument("--refresh-every", type=int, default=1)
+    ap.add_argument("--nsys", type=int, default=512)
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--duration", type=float, default=10.0)
+    ap.add_argument("--drain", type=float, default=20.0)
+    ap.add_argument("--serve-steps", type=int, default=100)
+    ap.add_argument("--serve-nmax", type=float, default=1e6)
+    ap.add_argument("--budget-gb", type=float, default=160.0)
+    ap.add_argument("--max-active", type=int, default=1 << 22)
+    ap.add_argument("--isolated-samples", type=int, default=8)
     ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -334,7 +590,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_gpu(args, cfg, rank, world, local_rank)
+        runner = {"c3": run_kdk, "c4": run_ensemble, "c5": run_serve}.get(args.config, run_gpu)
+        runner(args, cfg, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

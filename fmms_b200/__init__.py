@@ -65,6 +65,7 @@ class Config(C.Structure):
         ("m2l_kernel", C.c_int),
         ("device", C.c_int),
         ("stream", C.c_void_p),
+        ("p2p_tile", C.c_int),
     ]
 
 
@@ -183,7 +184,7 @@ class Fmm:
 
     def __init__(self, mass, pos, p: int = 8, eps: float = 1e-5, n_leaf: int = 16, *, mac: str = "dehnen",
                  theta: float = 0.5, softening: float = 0.0, precision: str = "plain", center: str = "com",
-                 m2l: str = "auto", device: int = 0, stream: int | None = None):
+                 m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0):
         cfg = Config()
         lib().fmmx_config_default(C.byref(cfg))
         cfg.p = int(p)
@@ -197,6 +198,7 @@ class Fmm:
         cfg.m2l_kernel = {"auto": M2L_AUTO, "naive": M2L_NAIVE, "rotation": M2L_ROTATION}[m2l]
         cfg.device = int(device)
         cfg.stream = stream
+        cfg.p2p_tile = int(p2p_tile)
         self.cfg = cfg
         self.p = cfg.p
         h = _vp()

@@ -480,11 +480,12 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
 fmmx_status walk_impl(fmmx_ctx* ctx) {
     cudaStream_t s = ctx->stream;
     const int nc = ctx->nc;
-    if (ctx->cap_front == 0) {
-        ctx->cap_front = (uint32_t)std::min<uint64_t>(64ull * nc + 1024, 0x7fffffffull);
-        ctx->cap_m2l = (uint32_t)std::min<uint64_t>(64ull * nc + 1024, 0x7fffffffull);
-        ctx->cap_p2p = (uint32_t)std::min<uint64_t>(32ull * nc + 1024, 0x7fffffffull);
-    }
+    // capacities follow the current tree (a context may see trees of very
+    // different sizes, e.g. the forests of a serving loop) and grow on overflow
+    auto at_least = [](uint32_t c, uint64_t w) { return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(c, w), 0x7fffffffull); };
+    ctx->cap_front = at_least(ctx->cap_front, 64ull * nc + 1024);
+    ctx->cap_m2l = at_least(ctx->cap_m2l, 64ull * nc + 1024);
+    ctx->cap_p2p = at_least(ctx->cap_p2p, 32ull * nc + 1024);
     CK(ctx->wcounts.ensure(WC_SIZE), "alloc");
     CK(ctx->wpops.ensure(1), "alloc");
     MacParams mp;
@@ -533,9 +534,9 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
         }
         if (!done) return fail(ctx, FMMX_TIMEOUT, "dual walk did not terminate");
         if (hc[WC_OVERFLOW]) {
-            if (attempt > 8) return fail(ctx, FMMX_OUT_OF_MEMORY, "walk capacity");
+            if (attempt > 24) return fail(ctx, FMMX_OUT_OF_MEMORY, "walk capacity");
             auto grow = [](uint32_t c, int used) {
-                uint64_t w2 = std::max<uint64_t>(2ull * c, (uint64_t)used + (uint64_t)used / 2 + 1024);
+                uint64_t w2 = std::max<uint64_t>(4ull * c, (uint64_t)used + (uint64_t)used / 2 + 1024);
                 return (uint32_t)std::min<uint64_t>(w2, 0x7fffffffull);
             };
             if (hc[WC_OVERFLOW] & 1) ctx->cap_front = grow(ctx->cap_front, 0);
@@ -626,9 +627,8 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     CKL("l2l (mixed)");
     if (tm) CK(cudaEventRecord(ev[7], s), "event");
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
-    k_p2p_mixed<<<std::min<unsigned>(nc, 148u * 16u), 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
-                                                                    ctx->m.p, soft2, ctx->nax.p, ctx->nay.p,
-                                                                    ctx->naz.p, ctx->npot.p);
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, std::min<unsigned>(nc, 148u * 16u), s, lp, nc, cv,
+                     ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s), "event");
     k_l2p_mixed<<<grid_for(n, 128), 128, 0, s>>>(n, ctx->body_leaf.p, ctx->order.p, cv, ctx->ell.p, p,
@@ -819,6 +819,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->m2l_kernel = FMMX_M2L_AUTO;
     c->device = 0;
     c->stream = nullptr;
+    c->p2p_tile = 0;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -849,6 +850,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (!(c.softening >= 0.0)) return FMMX_INVALID_ARG;
     if (c.center_mode != FMMX_CENTER_COM && c.center_mode != FMMX_CENTER_SPHERE) return FMMX_INVALID_ARG;
     if (c.precision != FMMX_PLAIN_FP64 && c.precision != FMMX_MIXED) return FMMX_INVALID_ARG;
+    if (c.p2p_tile < 0 || c.p2p_tile > 512) return FMMX_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

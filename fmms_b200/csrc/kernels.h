@@ -124,8 +124,9 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* body_leaf, const uint32_t* 
                             const double* ell, int p, const zf* loc, const double* x, const double* y,
                             const double* z, const double* nax, const double* nay, const double* naz,
                             const double* npot, double* acc, double* pot);
-__global__ void k_p2p_mixed(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,
-                            const double* m, float soft2, double* ax, double* ay, double* az, double* pot);
+void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, const double* x,
+                      const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
+                      double* az, double* pot);
 
 // p2p.cu
 __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,

@@ -329,7 +329,6 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
 // (hi, lo) accumulator with an error-free TwoSum. 1/r by rsqrt plus one
 // Newton step.
 #define P2PM_BLOCK 128
-#define P2PM_TILE 256
 #define P2PM_SRC_CHUNK 256
 
 struct DS {
@@ -343,6 +342,28 @@ __device__ __forceinline__ void ds_add(DS& a, float b) {
     a.lo += err;
 }
 
+// One source body against one target, FP32, d relative to the target leaf's
+// centre; rsqrt plus one Newton step.
+__device__ __forceinline__ void p2p_term(const float4 s, float xi, float yi, float zi, float soft2, float& ax,
+                                         float& ay, float& az, float& pt) {
+    const float dx = s.x - xi, dy = s.y - yi, dz = s.z - zi;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+    float inv = rsqrtf(r2);
+    inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
+    const float mi = s.w * inv;
+    const float f = mi * inv * inv;
+    ax = fmaf(f, dx, ax);
+    ay = fmaf(f, dy, ay);
+    az = fmaf(f, dz, az);
+    pt += mi;
+}
+
+// TILE: source bodies staged per shared-memory tile (the tile shape the
+// autotuner picks). Each thread carries two targets, so every staged source
+// feeds two interactions; groups of G threads cover the leaf's targets and
+// R = BLOCK / G groups split each tile. The target's own slot is skipped by
+// position only in the tiles that overlap the target leaf itself.
+template <int P2PM_TILE>
 __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv,
                                                          const double* __restrict__ x, const double* __restrict__ y,
                                                          const double* __restrict__ z, const double* __restrict__ m,
@@ -350,10 +371,11 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                                                          double* __restrict__ ay, double* __restrict__ az,
                                                          double* __restrict__ pot) {
     __shared__ float4 tb[P2PM_TILE];  // x, y, z relative to the target centre; mass
-    __shared__ uint32_t tslot[P2PM_TILE];
     __shared__ uint32_t pre[P2PM_SRC_CHUNK + 1];
     __shared__ uint32_t sfirst[P2PM_SRC_CHUNK];
-    __shared__ float red[8][P2PM_BLOCK];
+    __shared__ uint32_t wsum[P2PM_BLOCK / 32];
+    __shared__ int self_pos;
+    __shared__ float red[16][P2PM_BLOCK];
     const int tid = threadIdx.x;
     const int lane = tid & 31, wid = tid >> 5;
     for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
@@ -361,22 +383,30 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
         if (beg >= end) continue;
         const double cx = cv.cx[c], cy = cv.cy[c], cz = cv.cz[c];
         const uint32_t tf = cv.first[c], tn = cv.count[c];
-        for (uint32_t t0 = 0; t0 < tn; t0 += P2PM_BLOCK) {
-            const int nt = (int)min((uint32_t)P2PM_BLOCK, tn - t0);
-            const int R = P2PM_BLOCK / nt;
-            const int it = tid % nt, rep = tid / nt;
+        for (uint32_t t0 = 0; t0 < tn; t0 += 2 * P2PM_BLOCK) {
+            const int nt = (int)min((uint32_t)(2 * P2PM_BLOCK), tn - t0);
+            const int G = (nt + 1) >> 1;
+            const int R = P2PM_BLOCK / G;
+            const int g = tid % G, rep = tid / G;
             const bool active = rep < R;
-            const uint32_t islot = tf + t0 + it;
-            float xi = 0, yi = 0, zi = 0;
+            const int i0 = g, i1 = g + G;
+            const bool has1 = active && i1 < nt;
+            float x0 = 0, y0 = 0, z0 = 0, x1 = 0, y1 = 0, z1 = 0;
             if (active) {
-                xi = (float)(x[islot] - cx);
-                yi = (float)(y[islot] - cy);
-                zi = (float)(z[islot] - cz);
+                x0 = (float)(x[tf + t0 + i0] - cx);
+                y0 = (float)(y[tf + t0 + i0] - cy);
+                z0 = (float)(z[tf + t0 + i0] - cz);
             }
-            DS sax{0, 0}, say{0, 0}, saz{0, 0}, sp{0, 0};
+            if (has1) {
+                x1 = (float)(x[tf + t0 + i1] - cx);
+                y1 = (float)(y[tf + t0 + i1] - cy);
+                z1 = (float)(z[tf + t0 + i1] - cz);
+            }
+            DS a0x{0, 0}, a0y{0, 0}, a0z{0, 0}, p0{0, 0}, a1x{0, 0}, a1y{0, 0}, a1z{0, 0}, p1{0, 0};
             for (uint32_t sc = beg; sc < end; sc += P2PM_SRC_CHUNK) {
                 const int ns = (int)min((uint32_t)P2PM_SRC_CHUNK, end - sc);
                 __syncthreads();
+                if (tid == 0) self_pos = -1;
                 // exclusive prefix of source leaf sizes (warp scans, then warp totals)
                 for (int q0 = 0; q0 < ns; q0 += P2PM_BLOCK) {
                     const int q = q0 + tid;
@@ -391,81 +421,101 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                         const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
                         if (lane >= o) incl += t;
                     }
-                    __shared__ uint32_t wsum[P2PM_BLOCK / 32];
                     if (lane == 31) wsum[wid] = incl;
                     __syncthreads();
                     uint32_t base = q0 == 0 ? 0 : pre[q0];
                     for (int w = 0; w < wid; ++w) base += wsum[w];
-                    if (q < ns) pre[q + 1] = base + incl;
+                    if (q < ns) {
+                        pre[q + 1] = base + incl;
+                        if ((int)(L.keys[sc + q] & 0xffffffffu) == c) self_pos = (int)(base + incl - v);
+                    }
                     if (q0 == 0 && tid == 0) pre[0] = 0;
                     __syncthreads();
                 }
                 const uint32_t total = pre[ns];
+                const int sp = self_pos;  // position of the target leaf in this chunk's sources, or -1
                 for (uint32_t b0 = 0; b0 < total; b0 += P2PM_TILE) {
                     const uint32_t nb = min((uint32_t)P2PM_TILE, total - b0);
                     for (uint32_t t = tid; t < nb; t += P2PM_BLOCK) {
-                        const uint32_t g = b0 + t;
+                        const uint32_t gg = b0 + t;
                         int lo = 0, hi = ns;
                         while (hi - lo > 1) {
                             const int mid = (lo + hi) >> 1;
-                            if (pre[mid] <= g) lo = mid;
+                            if (pre[mid] <= gg) lo = mid;
                             else hi = mid;
                         }
-                        const uint32_t slot = sfirst[lo] + (g - pre[lo]);
+                        const uint32_t slot = sfirst[lo] + (gg - pre[lo]);
                         tb[t] = make_float4((float)(x[slot] - cx), (float)(y[slot] - cy), (float)(z[slot] - cz),
                                             (float)m[slot]);
-                        tslot[t] = slot;
                     }
                     __syncthreads();
                     if (active) {
-                        float pax = 0.f, pay = 0.f, paz = 0.f, pp = 0.f;
-                        for (uint32_t j = rep; j < nb; j += R) {
-                            const float4 s = tb[j];
-                            const float dx = s.x - xi, dy = s.y - yi, dz = s.z - zi;
-                            const bool self = tslot[j] == islot;  // the target itself: no term
-                            const float r2 = self ? 1.f : fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
-                            float inv = rsqrtf(r2);
-                            inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
-                            const float mj = self ? 0.f : s.w;
-                            const float mi = mj * inv;
-                            const float f = mi * inv * inv;
-                            pax = fmaf(f, dx, pax);
-                            pay = fmaf(f, dy, pay);
-                            paz = fmaf(f, dz, paz);
-                            pp += mi;
+                        float q0x = 0, q0y = 0, q0z = 0, q0p = 0, q1x = 0, q1y = 0, q1z = 0, q1p = 0;
+                        const bool overlaps = sp >= 0 && (uint32_t)sp < b0 + nb && (uint32_t)sp + tn > b0;
+                        if (!overlaps) {
+#pragma unroll 4
+                            for (uint32_t j = rep; j < nb; j += R) {
+                                const float4 sj = tb[j];
+                                p2p_term(sj, x0, y0, z0, soft2, q0x, q0y, q0z, q0p);
+                                p2p_term(sj, x1, y1, z1, soft2, q1x, q1y, q1z, q1p);
+                            }
+                        } else {
+                            // the target's own body sits at position sp + t0 + i in the sources
+                            const int s0 = sp + (int)t0 + i0 - (int)b0, s1 = sp + (int)t0 + i1 - (int)b0;
+                            for (uint32_t j = rep; j < nb; j += R) {
+                                float4 sj = tb[j];
+                                float4 sa = sj, sb = sj;
+                                if ((int)j == s0) sa = make_float4(x0 + 1.f, y0, z0, 0.f);  // no term
+                                if ((int)j == s1) sb = make_float4(x1 + 1.f, y1, z1, 0.f);
+                                p2p_term(sa, x0, y0, z0, soft2, q0x, q0y, q0z, q0p);
+                                p2p_term(sb, x1, y1, z1, soft2, q1x, q1y, q1z, q1p);
+                            }
                         }
-                        ds_add(sax, pax);
-                        ds_add(say, pay);
-                        ds_add(saz, paz);
-                        ds_add(sp, pp);
+                        ds_add(a0x, q0x);
+                        ds_add(a0y, q0y);
+                        ds_add(a0z, q0z);
+                        ds_add(p0, q0p);
+                        ds_add(a1x, q1x);
+                        ds_add(a1y, q1y);
+                        ds_add(a1z, q1z);
+                        ds_add(p1, q1p);
                     }
                     __syncthreads();
                 }
             }
-            red[0][tid] = sax.hi;
-            red[1][tid] = sax.lo;
-            red[2][tid] = say.hi;
-            red[3][tid] = say.lo;
-            red[4][tid] = saz.hi;
-            red[5][tid] = saz.lo;
-            red[6][tid] = sp.hi;
-            red[7][tid] = sp.lo;
+            red[0][tid] = a0x.hi; red[1][tid] = a0x.lo; red[2][tid] = a0y.hi; red[3][tid] = a0y.lo;
+            red[4][tid] = a0z.hi; red[5][tid] = a0z.lo; red[6][tid] = p0.hi; red[7][tid] = p0.lo;
+            red[8][tid] = a1x.hi; red[9][tid] = a1x.lo; red[10][tid] = a1y.hi; red[11][tid] = a1y.lo;
+            red[12][tid] = a1z.hi; red[13][tid] = a1z.lo; red[14][tid] = p1.hi; red[15][tid] = p1.lo;
             __syncthreads();
             if (tid < nt) {
-                double s[4] = {0, 0, 0, 0};
+                const int gi = tid % G, half = tid / G;  // target tid = gi + half * G
+                double sacc[4] = {0, 0, 0, 0};
                 for (int r = 0; r < R; ++r) {
-                    const int q = r * nt + tid;
-                    for (int k = 0; k < 4; ++k) s[k] += (double)red[2 * k][q] + (double)red[2 * k + 1][q];
+                    const int q = r * G + gi;
+                    for (int k = 0; k < 4; ++k)
+                        sacc[k] += (double)red[8 * half + 2 * k][q] + (double)red[8 * half + 2 * k + 1][q];
                 }
                 const uint32_t slot = tf + t0 + tid;
-                ax[slot] = s[0];
-                ay[slot] = s[1];
-                az[slot] = s[2];
-                pot[slot] = s[3];
+                ax[slot] = sacc[0];
+                ay[slot] = sacc[1];
+                az[slot] = sacc[2];
+                pot[slot] = sacc[3];
             }
             __syncthreads();
         }
     }
+}
+
+void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, const double* x,
+                      const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
+                      double* az, double* pot) {
+    if (tile <= 128)
+        k_p2p_mixed<128><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
+    else if (tile <= 256)
+        k_p2p_mixed<256><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
+    else
+        k_p2p_mixed<512><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
 }
 
 }  // namespace fmmx

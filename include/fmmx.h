@@ -71,6 +71,7 @@ typedef struct fmmx_config {
     int m2l_kernel;    /* fmmx_m2l_kernel */
     int device;        /* CUDA device ordinal */
     void* stream;      /* cudaStream_t to run on, or NULL for a private stream */
+    int p2p_tile;      /* source bodies per shared-memory tile of the mixed P2P (128, 256, 512; 0 = 256) */
 } fmmx_config;
 
 typedef struct fmmx_stats {
