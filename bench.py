@@ -513,16 +513,20 @@ def run_serve(args, cfg, rank, world, local_rank):
         sessions.append(Session(sid=i, mass=m, pos=p, vel=v, steps=args.serve_steps, dt=1e-3, arrival=float(t)))
     kw = dict(p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"], n_leaf=cfg["n_leaf"],
               precision=args.precision, budget_bytes=args.budget_gb * 1e9)
-    srv = Server(**kw)
+    srv = Server(**kw, latency_slo=args.latency_slo)  # calibrates the isolated step time first
     srv.start()  # every lane on its own thread and stream
     t0 = time.perf_counter()
     k = 0
+    occ = []  # (sessions, bodies) admitted, sampled every 2 ms while arrivals last
     while True:
         now = time.perf_counter() - t0
         while k < len(sessions) and sessions[k].arrival <= now:
             srv.submit(sessions[k])
             k += 1
-        if now > args.duration and (not srv.active or now > args.duration + args.drain):
+        if now <= args.duration:
+            act = srv.active
+            occ.append((len(act), sum(s.n for s in act)))
+        if now > args.duration and (not srv.busy() or now > args.duration + args.drain):
             break
         time.sleep(0.002)
     srv.stop()
@@ -531,13 +535,15 @@ def run_serve(args, cfg, rank, world, local_rank):
     rep["bodies_per_s"] = rep["bodies_stepped"] / wall
     # isolated step latency of completed sessions of every lane, against the mix
     ratios = []
-    picked = []
-    for ln in srv.lanes:
-        picked += [s for s in srv.done if srv.lane_for(s) is ln][: max(1, args.isolated_samples // len(srv.lanes))]
+    by_n = sorted(srv.done, key=lambda s: s.n)  # evenly spaced over the sizes that finished
+    picked = [by_n[i] for i in sorted({int(round(j)) for j in np.linspace(0, len(by_n) - 1, args.isolated_samples)})] \
+        if by_n else []
     for s in picked:
         _, _, alone_ms = run_session_alone(s, **kw)
-        ratios.append({"n": s.n, "mix_p99_ms": float(np.percentile(s.step_ms, 99)),
-                       "alone_p50_ms": float(np.percentile(alone_ms, 50))})
+        a50 = float(np.percentile(alone_ms, 50))
+        ratios.append({"n": s.n, "mix_p99_ms": float(np.percentile(s.step_ms, 99)), "alone_p50_ms": a50,
+                       "mix_p50_ms": float(np.percentile(s.step_ms, 50)), "mix_max_ms": float(np.max(s.step_ms)),
+                       "steps_over_2x": int(np.sum(np.asarray(s.step_ms) > 2 * a50)), "steps": len(s.step_ms)})
     rr = [r["mix_p99_ms"] / max(r["alone_p50_ms"], 1e-6) for r in ratios]
     line = {"metric": METRIC, "value": rep["bodies_per_s"], "unit": "bodies/s", "n_gpus": 1, "steps": rep["ticks"],
             "warmup": 0, "ms_per_step": rep["step_ms_p50"],
@@ -547,7 +553,9 @@ def run_serve(args, cfg, rank, world, local_rank):
                                    f"{args.serve_nmax:.0e}], {args.serve_steps} KDK steps", "budget_gb": args.budget_gb},
             "serve": {**rep, "wall_s": wall, "arrived": len(sessions), "submitted": k,
                       "queued_at_end": len(srv.queue), "active_at_end": len(srv.active),
-                      "lanes": [{"n_from": ln.lo, "batch_cap": ln.cap, "ticks": len(ln.tick_ms),
+                      "admitted_sessions_mean": float(np.mean([o[0] for o in occ])) if occ else 0.0,
+                      "admitted_bodies_mean": float(np.mean([o[1] for o in occ])) if occ else 0.0,
+                      "lanes": [{"n_from": ln.lo, "stream_priority": ln.priority, "ticks": len(ln.tick_ms),
                                  "tick_ms_p50": float(np.percentile(ln.tick_ms, 50)) if ln.tick_ms else None}
                                 for ln in srv.lanes],
                       "p99_over_isolated": {"median": float(np.median(rr)) if rr else None,
@@ -574,7 +582,8 @@ def main():
     ap.add_argument("--serve-steps", type=int, default=100)
     ap.add_argument("--serve-nmax", type=float, default=1e6)
     ap.add_argument("--budget-gb", type=float, default=160.0)
-    ap.add_argument("--isolated-samples", type=int, default=8)
+    ap.add_argument("--isolated-samples", type=int, default=10)
+    ap.add_argument("--latency-slo", type=float, default=2.0)
     ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")

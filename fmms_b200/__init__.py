@@ -66,6 +66,7 @@ class Config(C.Structure):
         ("device", C.c_int),
         ("stream", C.c_void_p),
         ("p2p_tile", C.c_int),
+        ("preemptible", C.c_int),
     ]
 
 
@@ -184,7 +185,8 @@ class Fmm:
 
     def __init__(self, mass, pos, p: int = 8, eps: float = 1e-5, n_leaf: int = 16, *, mac: str = "dehnen",
                  theta: float = 0.5, softening: float = 0.0, precision: str = "plain", center: str = "com",
-                 m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0):
+                 m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0,
+                 preemptible: bool = False):
         cfg = Config()
         lib().fmmx_config_default(C.byref(cfg))
         cfg.p = int(p)
@@ -199,6 +201,7 @@ class Fmm:
         cfg.device = int(device)
         cfg.stream = stream
         cfg.p2p_tile = int(p2p_tile)
+        cfg.preemptible = 1 if preemptible else 0
         self.cfg = cfg
         self.p = cfg.p
         h = _vp()

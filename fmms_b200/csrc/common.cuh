@@ -59,9 +59,12 @@ __host__ __device__ __forceinline__ cplx<T> zconj(cplx<T> a) {
 }
 
 // Per-order constants, uploaded once per context (engine.cu).
+// The tables cover every order up to FMMX_MAXP, so they are the same for all
+// contexts: a context created with another p re-uploads identical contents
+// and never changes the tables under a live context.
 struct OrderTables {
-    double fact[2 * FMMX_MAXP + 1];             // j!, j = 0..2p (moments.rs:11-17)
-    double binom[FMMX_MAXP + 1];                // C(p, k) (moments.rs:20-27)
+    double fact[2 * FMMX_MAXP + 1];             // j!, j = 0..2 FMMX_MAXP (moments.rs:11-17)
+    double binom[FMMX_MAXP + 1][FMMX_MAXP + 1]; // binom[p][k] = C(p, k) as p!/(k!(p-k)!) (moments.rs:20-27)
     double inv2m[FMMX_MAXP + 1];                // 1/(2m) (harmonic.rs:150)
     double invc[FMMX_MAXP + 1][FMMX_MAXP + 1];  // 1/(n^2 - m^2) (harmonic.rs:156,162)
 };

@@ -37,11 +37,20 @@ struct DBuf {
         p = nullptr;
         cap = 0;
     }
+    // Grows by at least half of the current capacity, so a context that sees
+    // slowly growing inputs (a serving loop's forests) reallocates -- and
+    // cudaFree synchronises the device -- only a logarithmic number of times.
     cudaError_t ensure(size_t n) {
         if (n <= cap && p) return cudaSuccess;
+        const size_t grown = cap + cap / 2;
         release();
-        size_t want = std::max<size_t>(n, 1);
+        size_t want = std::max<size_t>(std::max<size_t>(n, grown), 1);
         cudaError_t e = cudaMalloc((void**)&p, want * sizeof(T));
+        if (e != cudaSuccess && want > n) {  // no room for the slack: exactly n
+            cudaGetLastError();
+            want = std::max<size_t>(n, 1);
+            e = cudaMalloc((void**)&p, want * sizeof(T));
+        }
         if (e != cudaSuccess) {
             p = nullptr;
             cudaGetLastError();
@@ -280,13 +289,15 @@ void fmmx::make_rotw_tables(RotwTables& t) {
 
 namespace {
 
-void make_tables(int p, OrderTables& t) {
+void make_tables(OrderTables& t) {
+    const int P = FMMX_MAXP;
     std::memset(&t, 0, sizeof(t));
     t.fact[0] = 1.0;
-    for (int i = 1; i <= 2 * p; ++i) t.fact[i] = t.fact[i - 1] * (double)i;  // moments.rs:11-17
-    for (int k = 0; k <= p; ++k) t.binom[k] = t.fact[p] / (t.fact[k] * t.fact[p - k]);  // :20-27
-    for (int m = 1; m <= p; ++m) t.inv2m[m] = 1.0 / (double)(2 * m);
-    for (int n = 0; n <= p; ++n)
+    for (int i = 1; i <= 2 * P; ++i) t.fact[i] = t.fact[i - 1] * (double)i;  // moments.rs:11-17
+    for (int p = 0; p <= P; ++p)
+        for (int k = 0; k <= p; ++k) t.binom[p][k] = t.fact[p] / (t.fact[k] * t.fact[p - k]);  // :20-27
+    for (int m = 1; m <= P; ++m) t.inv2m[m] = 1.0 / (double)(2 * m);
+    for (int n = 0; n <= P; ++n)
         for (int m = 0; m < n; ++m) t.invc[n][m] = 1.0 / (double)(n * n - m * m);
 }
 
@@ -612,9 +623,13 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * H * sizeof(zf), s), "memset");
     if (ctx->n_m2l > 0) {
         if (p > kRotwMaxP) return fail(ctx, FMMX_INVALID_ARG, "mixed precision supports p <= 16");
-        CK(ctx->work.ensure(1), "alloc");
-        CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
-        CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, ctx->work.p, ctx->nsm, s), "m2l");
+        int* work = nullptr;  // preemptible: one block per destination cell
+        if (!ctx->cfg.preemptible) {
+            CK(ctx->work.ensure(1), "alloc");
+            CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
+            work = ctx->work.p;
+        }
+        CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, work, ctx->nsm, s), "m2l");
     }
     if (tm) CK(cudaEventRecord(ev[6], s), "event");
     LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 2);
@@ -627,7 +642,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     CKL("l2l (mixed)");
     if (tm) CK(cudaEventRecord(ev[7], s), "event");
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, std::min<unsigned>(nc, 148u * 16u), s, lp, nc, cv,
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)nc, s, lp, nc, cv,
                      ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s), "event");
@@ -740,9 +755,13 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         const unsigned g = std::min<unsigned>(nc, 148u * 16u);
         const M2lChoice ch = m2l_choice(ctx->cfg);
         if (ch == M2L_ROT_WARP) {
-            CK(ctx->work.ensure(1), "alloc");
-            CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
-            CK(launch_rotw_f64(p, lm, nc, cv, ctx->moments.p, ctx->locals.p, ctx->work.p, ctx->nsm, s), "m2l");
+            int* work = nullptr;  // preemptible: one block per destination cell
+            if (!ctx->cfg.preemptible) {
+                CK(ctx->work.ensure(1), "alloc");
+                CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(int), s), "memset");
+                work = ctx->work.p;
+            }
+            CK(launch_rotw_f64(p, lm, nc, cv, ctx->moments.p, ctx->locals.p, work, ctx->nsm, s), "m2l");
         } else if (ch == M2L_ROT_BLOCK) {
             const size_t smem = m2l_rot_smem_bytes(p);
             CK(cudaFuncSetAttribute(k_m2l_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
@@ -768,7 +787,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     if (tm) CK(cudaEventRecord(ev[7], s), "event");
     {
         const double soft2 = ctx->cfg.softening * ctx->cfg.softening;
-        k_p2p_f64<<<std::min<unsigned>(nc, 148u * 16u), 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
+        k_p2p_f64<<<(unsigned)nc, 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
                                                                       ctx->m.p, soft2, ctx->nax.p, ctx->nay.p,
                                                                       ctx->naz.p, ctx->npot.p);
         CKL("p2p");
@@ -820,6 +839,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->device = 0;
     c->stream = nullptr;
     c->p2p_tile = 0;
+    c->preemptible = 0;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -851,6 +871,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (c.center_mode != FMMX_CENTER_COM && c.center_mode != FMMX_CENTER_SPHERE) return FMMX_INVALID_ARG;
     if (c.precision != FMMX_PLAIN_FP64 && c.precision != FMMX_MIXED) return FMMX_INVALID_ARG;
     if (c.p2p_tile < 0 || c.p2p_tile > 512) return FMMX_INVALID_ARG;
+    if (c.preemptible != 0 && c.preemptible != 1) return FMMX_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -873,7 +894,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     ctx->events = true;
     for (int i = 0; i < 12; ++i) cudaEventCreate(&ctx->ev[i]);
     cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
-    make_tables(c.p, ctx->tab);
+    make_tables(ctx->tab);
     {
         RotwTables rt;
         make_rotw_tables(rt);

@@ -25,7 +25,7 @@ static cudaError_t launch_p(DirList L, int nc, CellsView cv, const float* scale,
     if (e != cudaSuccess) return e;
     int per_sm = (int)std::min<size_t>(32, (220 * 1024) / smem);
     if (per_sm < 1) per_sm = 1;
-    kern<<<nsm * per_sm, 32, smem, s>>>(L, nc, cv, scale, mom, loc, work);
+    kern<<<work ? nsm * per_sm : (unsigned)nc, 32, smem, s>>>(L, nc, cv, scale, mom, loc, work);
     return cudaGetLastError();
 }
 

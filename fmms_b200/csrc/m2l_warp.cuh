@@ -390,7 +390,10 @@ constexpr size_t rotw_smem_per_warp() {
     return (size_t)ROTW_LD * ((P + 1) * (P + 2) / 2 + (sizeof(T) == 4 ? 0 : 2 * (P + 1))) * sizeof(cplx<T>);
 }
 
-// Persistent warps pull destination cells from a counter.
+// One warp per block. With a work counter the warps are persistent and pull
+// destination cells from it; without one (work == nullptr) block b handles
+// destination cell b, so every block is short-lived and the block scheduler can
+// interleave kernels of higher-priority streams between them.
 template <typename T, int P, bool SCALED, bool FULL_LAYOUT>
 __global__ void __launch_bounds__(32) k_m2l_rotw(DirList L, int ncells, CellsView cv, const T* __restrict__ scale,
                                                 const cplx<T>* __restrict__ mom, cplx<T>* __restrict__ loc,
@@ -399,6 +402,13 @@ __global__ void __launch_bounds__(32) k_m2l_rotw(DirList L, int ncells, CellsVie
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw) + (size_t)wib * (rotw_smem_per_warp<T, P>() / sizeof(cplx<T>));
+    if (!work) {
+        const int c = blockIdx.x;
+        if (c >= ncells) return;
+        const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
+        if (beg < end) rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L.keys, cv, scale, mom, loc, sbuf, lane);
+        return;
+    }
     for (;;) {
         int c = 0;
         if (lane == 0) c = atomicAdd(work, 1);

@@ -730,7 +730,7 @@ __device__ __forceinline__ bool accept_dehnen(const CellsView& cv, const MacPara
     for (int j = 1; j <= p; ++j) rpows[j] = rpows[j - 1] * rb;
     const double* pw = pows + (size_t)a * (p + 1);
     double s = 0.0;
-    for (int k = 0; k <= p; ++k) s += c_tab.binom[k] * pw[k] * rpows[p - k];
+    for (int k = 0; k <= p; ++k) s += c_tab.binom[p][k] * pw[k] * rpows[p - k];
     const double ma = cv.mass[a];
     const double e = s / (ma * rp);
     const double denom = ra + rb;

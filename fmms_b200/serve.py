@@ -1,19 +1,43 @@
 """Serving loop: continuous batching of leapfrog sessions on one GPU.
 
 Sessions are N-body systems integrated with kick-drift-kick leapfrog. They
-arrive at any time, wait in a queue, and are admitted when the HBM budget
-allows. Admitted sessions are routed by size to lanes. A lane owns an engine
-context, a CUDA stream and (in threaded mode) a host thread, and advances its
-sessions one step per tick: the half kicks and drifts of all its sessions are
-one elementwise pass over their concatenated state, and their force
-evaluations are batched into ONE forest build + evaluation
-(fmmx_build_ensemble_device) -- one tree per session, no interaction across
-sessions, each session's result bitwise the one it gets alone. Sessions join a
-lane at its next tick and leave (freeing their memory) at the end of the tick
-that finishes them, so requests arriving while others run share the GPU. Lanes
-run concurrently on their own streams, so small sessions never wait behind the
-evaluation of large ones; within a lane the batch is capped so that a tick
-stays close to twice the isolated step time of its smallest session.
+arrive at any time, wait in a queue, and are admitted when the HBM budget and
+the latency target allow. A lane owns an engine context, a CUDA stream and, in
+threaded mode, a host thread, and advances its sessions one step per tick: the
+half kicks and drifts of all its sessions are one elementwise pass over their
+concatenated state, and their force evaluations are batched into ONE forest
+build + evaluation (fmmx_build_ensemble_device) -- one tree per session, no
+interaction across sessions, each session's result bitwise the one it gets
+alone. A session joins a lane by riding along in the lane's next forest
+evaluation with a zero time step (that evaluation gives its initial forces, so
+joining costs the others no extra pass), steps from the tick after, and leaves
+(freeing its memory) at the end of the tick that finishes it.
+
+Host<->device traffic stays off the step path: a submitted session's bodies are
+staged to the device on a copy stream by the submitting thread while it waits,
+and a finished session's final state is copied back to the host by a collector
+thread (in synchronous mode by `Server.collect`) while the lane goes on with
+its next tick.
+
+Latency: a session's step latency is the wall-clock interval between the ends
+of its consecutive steps; every step should take at most `latency_slo` times
+the step latency of the same session run alone. At start-up the server
+calibrates, for Plummer and uniform-cube systems of 1e3 .. 1e6 bodies, the
+isolated step latency and the extra latency of a second system of the same
+size in the same forest. A session is admitted only if the batch's latency
+predicted with it -- the batch's last measured step latency plus the session's
+calibrated extra latency (the larger of the two system types) -- stays within
+`headroom` times the isolated latency (the smaller of the two types) of the
+batch's smallest session, and only while the lane's recent steps stay within
+that bound (feedback against prediction error). The queue is scanned in arrival
+order and sessions that fit may overtake ones that do not, except a session
+that has waited longer than `max_bypass_s`: nobody overtakes it. Waiting time
+is reported apart from the step latency.
+
+By default there is one lane. Several lanes (`lanes`: lower bounds of N) run
+concurrently on streams of decreasing priority for increasing N; they share
+the GPU block by block, so each lane's ticks stretch by the others' work --
+more throughput at low load, weaker latency bounds.
 
 Every session's bodies, velocities and last accelerations stay resident on the
 device between its steps. No reference counterpart (the reference has no
@@ -23,25 +47,25 @@ serving component).
 from __future__ import annotations
 
 import dataclasses
+import sys
 import threading
 import time
 from collections import deque
 
 import numpy as np
 
-# Device bytes per body kept resident (pos, vel, acc, pot, mass: 11 FP64) and the
-# engine's working memory per body of a forest evaluation (tree, expansions,
+# Device bytes per body kept resident (pos, vel, acc, pot, mass, dt: 12 FP64) and
+# the engine's working memory per body of a forest evaluation (tree, expansions,
 # lists) at p=8, leaf 64 with headroom; plus a fixed part per session.
-RESIDENT_BYTES_PER_BODY = 88
+RESIDENT_BYTES_PER_BODY = 96
 ENGINE_BYTES_PER_BODY = 640
 SESSION_FIXED_BYTES = 1 << 20
+STAGED_BYTES_PER_BODY = 56  # pos, vel, mass staged on the device while queued
 
-# Size classes (lower bounds) of the lanes, and the batch cap of a lane:
-# a tick costs about T0 + B / RATE for B bodies, an isolated step of the
-# smallest member T0 + n_min / RATE, so B <= T0 * RATE + 2 n_min keeps the tick
-# within twice that isolated step.
-LANE_BOUNDS = (0, 4_000, 16_000, 64_000, 256_000)
-T0_RATE_BODIES = 60_000
+# Size classes (lower bounds of N) of the lanes: one lane by default.
+LANE_BOUNDS = (0,)
+# Sizes at which the latencies are calibrated.
+CALIBRATION_N = (1_000, 3_000, 10_000, 30_000, 100_000, 300_000, 1_000_000)
 
 
 @dataclasses.dataclass
@@ -53,13 +77,18 @@ class Session:
     steps: int
     dt: float
     arrival: float = 0.0
-    # filled by the server
+    # filled by the server (times are perf_counter seconds)
+    submitted_at: float | None = None
     admitted_at: float | None = None
     finished_at: float | None = None
     steps_done: int = 0
+    primed: bool = False
+    last_end: float = 0.0  # end of its last step (or of its joining tick)
     step_ms: list = dataclasses.field(default_factory=list)
     result_pos: np.ndarray | None = None
     result_vel: np.ndarray | None = None
+    staged: tuple | None = dataclasses.field(default=None, repr=False)  # device pos, vel, mass, ready event
+    pending: tuple | None = dataclasses.field(default=None, repr=False)  # device pos, vel copies, ready event
 
     @property
     def n(self) -> int:
@@ -68,119 +97,233 @@ class Session:
     def bytes_needed(self) -> int:
         return self.n * (RESIDENT_BYTES_PER_BODY + ENGINE_BYTES_PER_BODY) + SESSION_FIXED_BYTES
 
+    def fresh(self) -> "Session":
+        """The same request, not yet served."""
+        return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
+                                   primed=False, last_end=0.0, step_ms=[], result_pos=None, result_vel=None,
+                                   staged=None, pending=None)
+
+
+def _interp_loglog(ns, vals, n):
+    ln = np.log(np.asarray(ns, dtype=np.float64))
+    lv = np.log(np.maximum(np.asarray(vals, dtype=np.float64), 1e-4))
+    x = np.log(max(float(n), 1.0))
+    if x >= ln[-1] and len(ln) > 1:
+        slope = max((lv[-1] - lv[-2]) / (ln[-1] - ln[-2]), 0.0)
+        return float(np.exp(lv[-1] + slope * (x - ln[-1])))
+    return float(np.exp(np.interp(x, ln, lv)))
+
+
+class LatencyModel:
+    """Calibrated step latencies (ms) against N: `iso(n)` the isolated step
+    latency, `extra(n)` the added latency of one more system of n bodies in a
+    forest. Log-log interpolation, extrapolated with the end slope."""
+
+    def __init__(self, ns, iso_ms, extra_ms):
+        self.ns = [int(n) for n in ns]
+        self.iso_ms = [float(v) for v in np.maximum.accumulate(np.asarray(iso_ms, dtype=np.float64))]
+        self.extra_ms = [max(float(v), 1e-3) for v in np.maximum.accumulate(np.asarray(extra_ms, dtype=np.float64))]
+
+    def iso(self, n) -> float:
+        return _interp_loglog(self.ns, self.iso_ms, n)
+
+    def extra(self, n) -> float:
+        return _interp_loglog(self.ns, self.extra_ms, n)
+
+    def table(self):
+        return [[n, round(a, 3), round(b, 3)] for n, a, b in zip(self.ns, self.iso_ms, self.extra_ms)]
+
 
 class Lane:
     """One size class: its own context and stream, continuous batching."""
 
-    def __init__(self, server: "Server", lo: int, cap_bodies: int):
+    def __init__(self, server: "Server", lo: int, priority: int = 0, preemptible: bool = False):
         torch = server.torch
         self.srv = server
         self.lo = lo
-        self.cap = cap_bodies
-        self.stream = torch.cuda.Stream(device=server.device)
+        self.priority = priority
+        self.stream = torch.cuda.Stream(device=server.device, priority=priority)
         self.fmm = server.fx.Fmm(None, None, server.p, 0.0, server.n_leaf, mac="theta", theta=server.theta,
                                  softening=server.softening, precision=server.precision, device=server.device,
-                                 stream=self.stream.cuda_stream)
+                                 stream=self.stream.cuda_stream, preemptible=preemptible)
         self.queue: deque[Session] = deque()
-        self.active: list[Session] = []
-        self.state = None  # pos, vel, acc, pot, mass of the active sessions (device)
-        self.tick_ms: list[float] = []
+        self.members: list[Session] = []  # primed (stepping) and joining sessions, in row order
+        self.state = None  # pos, vel, acc, pot, mass of the members (device)
+        self.dts = None  # per-row time step of the members; 0 for rows joining this tick
+        self.tick_ms: list[float] = []  # device time of each tick
+        self.last_interval_ms = None  # wall interval of the last tick that stepped sessions
+        self.predicted_ms = None  # predicted interval after the last admission, until measured
+        self.recent_ratio: deque[float] = deque(maxlen=8)
         self.bodies_stepped = 0
 
-    def offsets(self, sessions):
+    # ---------------------------------------------------------------- helpers
+    @staticmethod
+    def offsets(sessions):
         return np.concatenate([[0], np.cumsum([s.n for s in sessions])]).astype(np.uint64)
+
+    @property
+    def stepping(self):
+        return [s for s in self.members if s.primed]
+
+    def bodies(self):
+        return sum(s.n for s in self.members)
 
     def evaluate(self, pos, mass, acc, pot, offsets):
         self.fmm.build_ensemble_device(offsets, pos.data_ptr(), mass.data_ptr())
         self.fmm.evaluate_device(pos.data_ptr(), mass.data_ptr(), acc.data_ptr(), pot.data_ptr())
 
+    # ---------------------------------------------------------------- admission
     def admit(self, now):
+        srv = self.srv
+        model = srv.model
         new = []
-        bodies = sum(s.n for s in self.active)
-        while self.queue:
-            s = self.queue[0]
-            if (self.active or new) and bodies + s.n > self.cap:
-                break
-            if not self.srv.reserve(s.bytes_needed()):
-                break
-            self.queue.popleft()
-            s.admitted_at = now
-            new.append(s)
-            bodies += s.n
+        if not srv.gate_open(self):
+            return new
+        # predicted step latency of the batch as it stands, and its smallest member
+        tau = self.predicted_ms if self.predicted_ms is not None else self.last_interval_ms
+        nmin = min((s.n for s in self.members), default=None)
+        for s in list(self.queue)[: srv.scan]:
+            pred = None
+            fits = True
+            if model is not None and nmin is not None:
+                pred = (tau if tau is not None else model.iso(nmin)) + model.extra(s.n)
+                fits = pred <= srv.headroom * model.iso(min(nmin, s.n))
+            if fits and srv.reserve(s.bytes_needed()):
+                self.queue.remove(s)
+                s.admitted_at = now
+                new.append(s)
+                if model is not None:
+                    tau = model.iso(s.n) if pred is None else pred
+                nmin = s.n if nmin is None else min(nmin, s.n)
+                continue
+            if model is None or (s.submitted_at is not None and now - s.submitted_at > srv.max_bypass_s):
+                break  # first come, first served from this session on
+        if new and model is not None:
+            self.predicted_ms = tau
         return new
 
     def join(self, new):
-        torch = self.srv.torch
+        """Append the new sessions' rows with a zero time step."""
         if not new:
             return
-        dev = self.srv.dev
-        pos = torch.from_numpy(np.concatenate([s.pos for s in new])).to(dev, non_blocking=False)
-        vel = torch.from_numpy(np.concatenate([s.vel for s in new])).to(dev)
-        mass = torch.from_numpy(np.concatenate([s.mass for s in new])).to(dev)
-        acc = torch.empty_like(pos)
-        pot = torch.empty_like(mass)
-        self.evaluate(pos, mass, acc, pot, self.offsets(new))
-        if self.state is None:
-            self.state = [pos, vel, acc, pot, mass]
-        else:
-            self.state = [torch.cat([a, b]) for a, b in zip(self.state, [pos, vel, acc, pot, mass])]
-        self.active.extend(new)
+        torch = self.srv.torch
+        for s in new:
+            if s.staged is None:
+                self.srv.stage(s)
+            self.stream.wait_event(s.staged[3])
+        pos = torch.cat([s.staged[0] for s in new])
+        vel = torch.cat([s.staged[1] for s in new])
+        mass = torch.cat([s.staged[2] for s in new])
+        for s in new:
+            for t in s.staged[:3]:
+                t.record_stream(self.stream)
+            s.staged = None
+        self.srv.unstage(sum(s.n for s in new))
+        acc = torch.zeros_like(pos)
+        pot = torch.zeros_like(mass)
+        rows = [pos, vel, acc, pot, mass]
+        self.state = rows if self.state is None else [torch.cat([a, b]) for a, b in zip(self.state, rows)]
+        self.members.extend(new)
+        self._set_dts()
+
+    def _set_dts(self):
+        torch = self.srv.torch
+        if not self.members:
+            self.dts = None
+            return
+        d = np.concatenate([np.full(s.n, s.dt if s.primed else 0.0) for s in self.members])
+        self.dts = torch.from_numpy(d).to(self.srv.dev)[:, None]
 
     def leave(self, now):
         torch = self.srv.torch
-        keep, rows = [], []
-        off = self.offsets(self.active)
+        keep, rows, out = [], [], []
+        off = self.offsets(self.members)
         pos, vel = self.state[0], self.state[1]
-        for i, s in enumerate(self.active):
+        for i, s in enumerate(self.members):
             a, b = int(off[i]), int(off[i + 1])
             if s.steps_done >= s.steps:
-                s.result_pos = pos[a:b].cpu().numpy()
-                s.result_vel = vel[a:b].cpu().numpy()
-                s.finished_at = now
-                self.srv.release(s.bytes_needed())
-                self.srv.finished(s)
+                out.append((s, pos[a:b].clone(), vel[a:b].clone()))
             else:
                 keep.append(s)
                 rows.append(torch.arange(a, b, device=self.srv.dev))
-        self.active = keep
+        for s, p, v in out:
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            s.pending = (p, v, ev)
+            s.finished_at = now
+            self.srv.release(s.bytes_needed())
+            self.srv.finished(s)
+        changed = bool(out)
+        self.members = keep
         if not keep:
             self.state = None
-            return
-        idx = torch.cat(rows)
-        self.state = [t.index_select(0, idx) for t in self.state]
+            self.dts = None
+            self.recent_ratio.clear()
+            self.last_interval_ms = None
+            self.predicted_ms = None
+            return changed
+        if changed:
+            idx = torch.cat(rows)
+            self.state = [t.index_select(0, idx) for t in self.state]
+        return changed
 
+    # ---------------------------------------------------------------- one tick
     def tick(self) -> float:
         torch = self.srv.torch
         with torch.cuda.stream(self.stream):
             self.join(self.admit(time.perf_counter()))
-            if not self.active:
+            if not self.members:
                 return 0.0
+            stepping = self.stepping
             pos, vel, acc, pot, mass = self.state
-            dts = torch.from_numpy(np.concatenate([np.full(s.n, s.dt) for s in self.active])).to(self.srv.dev)[:, None]
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(self.stream)
-            vel.add_(0.5 * dts * acc)
-            pos.add_(dts * vel)
-            self.evaluate(pos, mass, acc, pot, self.offsets(self.active))
-            vel.add_(0.5 * dts * acc)
+            if stepping:
+                vel.add_(0.5 * self.dts * acc)
+                pos.add_(self.dts * vel)
+            self.evaluate(pos, mass, acc, pot, self.offsets(self.members))
+            if stepping:
+                vel.add_(0.5 * self.dts * acc)
             e1.record(self.stream)
             e1.synchronize()
+            t_end = time.perf_counter()
             ms = e0.elapsed_time(e1)
             self.tick_ms.append(ms)
-            for s in self.active:
+            for s in stepping:
                 s.steps_done += 1
-                s.step_ms.append(ms)
+                s.step_ms.append(1e3 * (t_end - s.last_end))
+                s.last_end = t_end
                 self.bodies_stepped += s.n
-            self.leave(time.perf_counter())
+            if stepping:
+                self.last_interval_ms = max(s.step_ms[-1] for s in stepping)
+                self.predicted_ms = None
+                if self.srv.model is not None:
+                    self.recent_ratio.append(max(s.step_ms[-1] / self.srv.model.iso(s.n) for s in stepping))
+            joined = [s for s in self.members if not s.primed]
+            for s in joined:
+                s.primed = True
+                s.last_end = t_end
+            changed = self.leave(time.perf_counter())
+            if joined or changed:
+                self._set_dts()
             return ms
 
 
 class Server:
-    """Front end: HBM admission, routing to lanes, synchronous or threaded."""
+    """Front end: HBM and latency admission, routing to lanes, synchronous or
+    threaded driving.
+
+    latency_slo: target ratio of a step's latency to the session's isolated
+    step latency; None turns latency admission off (first come, first served
+    under the HBM budget only).
+    headroom: the bound used for admission decisions (below latency_slo, to
+    leave room for prediction error).
+    """
 
     def __init__(self, *, p=8, theta=0.5, softening=1e-3, n_leaf=64, precision="mixed", budget_bytes=160e9,
-                 lanes=LANE_BOUNDS, device=0, max_active_bodies=None):
+                 lanes=LANE_BOUNDS, device=0, latency_slo=None, headroom=None, model=None, max_bypass_s=2.0,
+                 scan=256, stage_limit_bytes=8e9):
         import torch
 
         import fmms_b200 as fx
@@ -193,17 +336,75 @@ class Server:
         self.p, self.theta, self.softening, self.n_leaf, self.precision = p, theta, softening, n_leaf, precision
         self.budget = float(budget_bytes)
         self.used = 0.0
+        self.staged_bytes = 0.0
+        self.stage_limit = float(stage_limit_bytes)
         self.lock = threading.Lock()
-        bounds = tuple(lanes)
+        self.latency_slo = latency_slo
+        self.headroom = headroom if headroom is not None else (0.8 * latency_slo if latency_slo else None)
+        self.max_bypass_s = max_bypass_s
+        self.scan = scan
+        self.copy_stream = torch.cuda.Stream(device=device)
+        bounds = tuple(sorted(lanes))
+        try:
+            least, greatest = torch.cuda.Stream.priority_range()
+        except Exception:  # noqa: BLE001 - no priorities: every lane at the default
+            least, greatest = 0, 0
         self.lanes = []
         for i, lo in enumerate(bounds):
-            cap = T0_RATE_BODIES + 2 * max(lo, 1000)
-            if max_active_bodies is not None:
-                cap = min(cap, max_active_bodies) if i < len(bounds) - 1 else max(cap, 1)
-            self.lanes.append(Lane(self, lo, cap))
+            prio = max(greatest, least - (len(bounds) - 1 - i)) if greatest < least else least
+            # with several lanes, short M2L blocks let the higher-priority lanes in
+            self.lanes.append(Lane(self, lo, prio, preemptible=len(bounds) > 1))
         self.done: list[Session] = []
+        self.outstanding = 0
         self._threads = []
         self._stop = threading.Event()
+        self._switch = None
+        self.model = None
+        if latency_slo is not None:
+            self.model = model if model is not None else self.calibrate()
+
+    # -------------------------------------------------------------- calibration
+    def _run_batch(self, sessions):
+        """Run sessions to completion as one batch in the lane of the first
+        (synchronously); the median step latency without the first two steps
+        (which may grow the lane's buffers)."""
+        ln = self.lane_for(sessions[0])
+        assert not ln.members and not ln.queue
+        for s in sessions:
+            self.submit(s, lane=ln)
+        while ln.members or ln.queue:
+            ln.tick()
+        self.collect(sessions)
+        for s in sessions:
+            self.done.remove(s)
+        return float(np.median(sessions[0].step_ms[2:]))
+
+    def calibrate(self, ns=CALIBRATION_N, steps=5) -> LatencyModel:
+        """Isolated step latency and the extra latency of a second system of
+        the same size, for Plummer and uniform-cube systems of each size."""
+        iso, extra = [], []
+        for i, n in enumerate(ns):
+            iso_t, ext_t = [], []
+            for kind in ("plummer", "uniform"):
+                pair = []
+                for j in range(2):
+                    seed = 90_000 + 10 * i + j
+                    if kind == "plummer":
+                        mass, pos, vel = self.fx.gen_plummer_ic(int(n), 1.0, 1.0, 20.0, seed)
+                    else:
+                        mass, pos = self.fx.gen_uniform_lognormal(int(n), 0.5, seed)
+                        vel = np.zeros_like(pos)
+                    pair.append(Session(sid=-1, mass=mass, pos=pos, vel=vel, steps=steps, dt=1e-3))
+                one = self._run_batch([pair[0]])
+                two = self._run_batch([pair[0].fresh(), pair[1]])
+                iso_t.append(one)
+                ext_t.append(two - one)
+            iso.append(min(iso_t))
+            extra.append(max(ext_t))
+        for ln in self.lanes:
+            ln.tick_ms.clear()
+            ln.bodies_stepped = 0
+        return LatencyModel(ns, iso, extra)
 
     # -------------------------------------------------------------- memory
     def reserve(self, nbytes) -> bool:
@@ -220,9 +421,52 @@ class Server:
     def mem_used(self) -> float:
         return self.used
 
+    def stage(self, s: Session):
+        """Bodies of a waiting session to the device on the copy stream (the
+        calling thread waits for the copy; no pinned allocations); the copy's
+        event orders their use on a lane's stream."""
+        torch = self.torch
+        with torch.cuda.stream(self.copy_stream):
+            dev = [torch.from_numpy(np.ascontiguousarray(a)).to(self.dev) for a in (s.pos, s.vel, s.mass)]
+            ev = torch.cuda.Event()
+            ev.record(self.copy_stream)
+        s.staged = (dev[0], dev[1], dev[2], ev)
+        with self.lock:
+            self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+
+    def unstage(self, n_bodies):
+        with self.lock:
+            self.staged_bytes -= n_bodies * STAGED_BYTES_PER_BODY
+
+    def collect(self, sessions=None):
+        """Copy the final state of finished sessions to the host (on the copy
+        stream, after the lane's stream produced it) and fill their results."""
+        torch = self.torch
+        for s in list(self.done if sessions is None else sessions):
+            pend = s.pending
+            if pend is None:
+                continue
+            p, v, ev = pend
+            self.copy_stream.wait_event(ev)
+            with torch.cuda.stream(self.copy_stream):
+                s.result_pos = p.cpu().numpy()
+                s.result_vel = v.cpu().numpy()
+            s.pending = None
+
     def finished(self, s):
         with self.lock:
             self.done.append(s)
+            self.outstanding -= 1
+
+    def busy(self) -> bool:
+        """Sessions submitted and not finished (queued, joining or stepping)."""
+        return self.outstanding > 0
+
+    def gate_open(self, lane) -> bool:
+        """Admission feedback: the lane's recent steps within the headroom."""
+        if self.model is None:
+            return True
+        return not lane.recent_ratio or max(lane.recent_ratio) <= self.headroom
 
     # -------------------------------------------------------------- routing
     def lane_for(self, s: Session) -> Lane:
@@ -232,13 +476,17 @@ class Server:
                 lane = ln
         return lane
 
-    def submit(self, s: Session):
+    def submit(self, s: Session, lane=None):
+        s.submitted_at = time.perf_counter()
+        if self.staged_bytes + s.n * STAGED_BYTES_PER_BODY <= self.stage_limit:
+            self.stage(s)
         with self.lock:
-            self.lane_for(s).queue.append(s)
+            self.outstanding += 1
+            (lane or self.lane_for(s)).queue.append(s)
 
     @property
     def active(self):
-        return [s for ln in self.lanes for s in ln.active]
+        return [s for ln in self.lanes for s in ln.members]
 
     @property
     def queue(self):
@@ -248,14 +496,15 @@ class Server:
     def tick(self):
         """Synchronous mode: one tick of every lane that has work."""
         for ln in self.lanes:
-            if ln.active or ln.queue:
+            if ln.members or ln.queue:
                 ln.tick()
 
     def run_until_idle(self, max_ticks=1 << 30):
         t = 0
-        while (self.active or self.queue) and t < max_ticks:
+        while self.busy() and t < max_ticks:
             self.tick()
             t += 1
+        self.collect()
 
     def start(self):
         """Threaded mode: every lane ticks on its own host thread and stream."""
@@ -263,15 +512,29 @@ class Server:
         def loop(ln):
             self.torch.cuda.set_device(self.device)
             while not self._stop.is_set():
-                if ln.active or ln.queue:
+                if ln.members or ln.queue:
                     ln.tick()
-                else:
+                if not ln.members:  # idle, or admission refused: do not spin on the GIL
                     time.sleep(0.0005)
 
+        def collector():
+            self.torch.cuda.set_device(self.device)
+            while not self._stop.is_set():
+                self.collect()
+                time.sleep(0.005)
+
+        # lane threads hand the interpreter lock to each other and to the
+        # submitting thread between short pieces of host work; the default 5 ms
+        # switch interval would add up to that much to a step
+        self._switch = sys.getswitchinterval()
+        sys.setswitchinterval(2e-4)
         for ln in self.lanes:
             th = threading.Thread(target=loop, args=(ln,), daemon=True)
             th.start()
             self._threads.append(th)
+        th = threading.Thread(target=collector, daemon=True)
+        th.start()
+        self._threads.append(th)
 
     def stop(self):
         self._stop.set()
@@ -279,21 +542,36 @@ class Server:
             th.join()
         self._threads = []
         self._stop.clear()
+        if self._switch is not None:
+            sys.setswitchinterval(self._switch)
+            self._switch = None
+        self.collect()
 
     def report(self) -> dict:
         sess = self.done + self.active
         lat = np.array([m for s in sess for m in s.step_ms]) if sess else np.array([0.0])
+        waits = np.array([1e3 * (s.admitted_at - s.submitted_at) for s in sess
+                          if s.admitted_at is not None and s.submitted_at is not None])
         busy = max((sum(ln.tick_ms) for ln in self.lanes), default=0.0) * 1e-3
         stepped = sum(ln.bodies_stepped for ln in self.lanes)
-        return {"sessions_done": len(self.done), "ticks": sum(len(ln.tick_ms) for ln in self.lanes),
-                "step_ms_p50": float(np.percentile(lat, 50)), "step_ms_p99": float(np.percentile(lat, 99)),
-                "bodies_stepped": stepped, "lane_busy_s_max": busy}
+        out = {"sessions_done": len(self.done), "ticks": sum(len(ln.tick_ms) for ln in self.lanes),
+               "step_ms_p50": float(np.percentile(lat, 50)), "step_ms_p99": float(np.percentile(lat, 99)),
+               "bodies_stepped": stepped, "lane_busy_s_max": busy}
+        if len(waits):
+            out["admission_wait_ms_p50"] = float(np.percentile(waits, 50))
+            out["admission_wait_ms_p99"] = float(np.percentile(waits, 99))
+        if self.model is not None:
+            out["latency_slo"] = self.latency_slo
+            out["headroom"] = self.headroom
+            out["calibration_n_iso_extra_ms"] = self.model.table()
+        return out
 
 
 def run_session_alone(sess: Session, **kw) -> tuple[np.ndarray, np.ndarray, list]:
     """The same session through its own server, for alone-vs-mix checks."""
+    kw = {k: v for k, v in kw.items() if k not in ("latency_slo", "headroom", "model")}
     srv = Server(**kw)
-    srv.submit(dataclasses.replace(sess, step_ms=[], steps_done=0, result_pos=None, result_vel=None))
+    srv.submit(sess.fresh())
     srv.run_until_idle()
     d = srv.done[0]
     return d.result_pos, d.result_vel, d.step_ms
