@@ -63,16 +63,25 @@ def make_inputs(fx, cfg):
 def m2l_flops_per_translation(p: int, kernel: str) -> float:
     """Flops (FMA = 2) of one directed M2L translation as the kernel runs it.
 
-    rotation (warp kernel, m >= 0 half basis): per degree of K = k+1 terms the
-    back rotation costs 8K^2 + 13K and the forward 8K^2 + 12K; the axial
-    translation 4 per (n, m, k) term plus 4 per output; the lane reduction 2
-    per output; phases and geometry about 12(p+1) + 50.
+    rotation (warp kernel, m >= 0 half basis): per degree k (K = k+1 terms)
+    four real swap products, each 2 flops per structurally nonzero entry of
+    its two (K x K) half-basis matrices (about half the entries: Pm[r][q] != 0
+    needs r + q + k even, Qm[r][q] != 0 needs r, q >= 1 and r + q + k odd),
+    plus 25K for phases and scaling; the axial translation 4 per (n, m, k)
+    term plus 4 per output; the lane reduction 2 per output; phases and
+    geometry about 12(p+1) + 50.
     naive: 8 per complex term of sum_{n,m} (p-n+1)^2 (translate.rs:47-136).
     """
     if kernel == "naive":
         return 8.0 * sum((2 * n + 1) * (p - n + 1) ** 2 for n in range(p + 1))
     h = (p + 1) * (p + 2) // 2
-    rot = sum(16 * K * K + 25 * K for K in range(1, p + 2))
+
+    def nz(k):  # structural nonzeros of Pm and Qm of degree k
+        r = range(k + 1)
+        return (sum(1 for a in r for b in r if (a + b + k) % 2 == 0)
+                + sum(1 for a in r for b in r if a >= 1 and b >= 1 and (a + b + k) % 2 == 1))
+
+    rot = sum(8 * nz(k) + 25 * (k + 1) for k in range(p + 1))
     axial = sum(max(0, p - n - m + 1) for m in range(p + 1) for n in range(m, p + 1))
     return rot + 4 * axial + 6 * h + 12 * (p + 1) + 50
 

@@ -287,6 +287,22 @@ void fmmx::make_rotw_tables(RotwTables& t) {
         }
 }
 
+bool fmmx::rotw_tables_check(const RotwTables& t) {
+    for (int k = 0; k <= kRotwMaxP; ++k) {
+        const int n = k + 1;
+        const double* m = t.mats.data() + rot_moff_host(k);  // P, Q, PT, QT
+        for (int r = 0; r < n; ++r)
+            for (int q = 0; q < n; ++q) {
+                const bool p_nz = ((r + q + k) & 1) == 0;
+                const bool q_nz = r >= 1 && q >= 1 && ((r + q + k) & 1) == 1;
+                if (!p_nz && (m[r * n + q] != 0.0 || m[2 * n * n + r * n + q] != 0.0)) return false;
+                if (q >= 1 && !q_nz && (m[n * n + r * n + q] != 0.0 || m[3 * n * n + r * n + q] != 0.0))
+                    return false;
+            }
+    }
+    return true;
+}
+
 namespace {
 
 void make_tables(OrderTables& t) {
@@ -898,6 +914,10 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     {
         RotwTables rt;
         make_rotw_tables(rt);
+        if (!rotw_tables_check(rt)) {  // cannot happen: the tables are fixed numbers
+            fmmx_destroy(ctx);
+            return FMMX_DEVICE_ERROR;
+        }
         rotw_upload_f64(rt, ctx->stream);
         rotw_upload_f32(rt, ctx->stream);
     }

@@ -89,23 +89,6 @@ __device__ __forceinline__ void mul_i_pow(T& r, T& i) {
     else if constexpr ((M & 3) == 3) { r = b; i = -a; }
 }
 
-// Real half-basis swap matvec: Re(s) = Pm Re(v), Im(s) = Qm Im(v).
-template <typename T, int N, int OFF>
-__device__ __forceinline__ void swap_matvec(const T (&vr)[N], const T (&vi)[N], T (&sr)[N], T (&si)[N]) {
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-        T a = c_rot[OFF + r * N] * vr[0];
-        T b = T(0);
-#pragma unroll
-        for (int q = 1; q < N; ++q) {
-            a += c_rot[OFF + r * N + q] * vr[q];
-            b += c_rot[OFF + N * N + r * N + q] * vi[q];
-        }
-        sr[r] = a;
-        si[r] = b;
-    }
-}
-
 template <int M, typename T, int N>
 struct Unroll {  // compile-time loop helper: f(integral_constant<m>) for m = M..N-1
     template <class F>
@@ -116,6 +99,28 @@ struct Unroll {  // compile-time loop helper: f(integral_constant<m>) for m = M.
         }
     }
 };
+
+// Real half-basis swap matvec: Re(s) = Pm Re(v), Im(s) = Qm Im(v), degree
+// K = N - 1. The half-basis swap matrices are zero in a parity pattern:
+// Pm[r][q] = 0 unless r + q + K is even, Qm[r][q] = 0 unless r, q >= 1 and
+// r + q + K is odd, and the same for the matrices of B_K^T (rotw_tables_check
+// verifies this on the host for every degree when a context is created). The
+// zero terms, about half of each product, are left out at compile time; the
+// others are added in the same order as in the full product.
+template <typename T, int N, int OFF>
+__device__ __forceinline__ void swap_matvec(const T (&vr)[N], const T (&vi)[N], T (&sr)[N], T (&si)[N]) {
+    Unroll<0, T, N>::run([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        T a = T(0), b = T(0);
+        Unroll<0, T, N>::run([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (((r + q + N - 1) & 1) == 0) a += c_rot[OFF + r * N + q] * vr[q];
+            if constexpr (r >= 1 && q >= 1 && ((r + q + N - 1) & 1) == 1) b += c_rot[OFF + N * N + r * N + q] * vi[q];
+        });
+        sr[r] = a;
+        si[r] = b;
+    });
+}
 
 template <typename T, int P, int K, bool FULL_LAYOUT, class PH>
 __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,

@@ -15,6 +15,8 @@ struct RotwTables {
     std::vector<double> mats, fm, ifm, fact;
 };
 void make_rotw_tables(RotwTables& t);
+// true if the tables have the zero pattern the warp kernel relies on
+bool rotw_tables_check(const RotwTables& t);
 void rotw_upload_f64(const RotwTables& t, cudaStream_t s);
 void rotw_upload_f32(const RotwTables& t, cudaStream_t s);
 cudaError_t launch_rotw_f64(int p, DirList L, int nc, CellsView cv, const zd* mom, zd* loc, int* work, int nsm,
