@@ -596,8 +596,12 @@ def main():
     ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--n", type=int, default=0, help="override N (small cases for profiling)")
     args = ap.parse_args()
-    cfg = CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config]
+    cfg = dict(CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config])
+    if args.n > 0:
+        cfg["n"] = args.n
+        cfg["workload"] += f" (N overridden: {args.n})"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

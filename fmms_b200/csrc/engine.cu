@@ -143,6 +143,7 @@ struct fmmx_ctx {
 
     // directed lists
     DBuf<uint64_t> m2l_keys, m2l_keys_s, p2p_keys, p2p_keys_s;
+    int list_shift = 32;  // keys of the directed lists: (dst << list_shift) | src
     DBuf<uint32_t> m2l_seg_b, m2l_seg_e, p2p_seg_b, p2p_seg_e;
 
     DBuf<int> work;  // persistent-kernel work counter
@@ -581,7 +582,9 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
 fmmx_status lists_impl(fmmx_ctx* ctx) {
     cudaStream_t s = ctx->stream;
     const int nc = ctx->nc;
-    const int cbits = 32 + bits_for((uint64_t)nc);
+    const int shift = bits_for((uint64_t)nc);  // keys (dst << shift) | src
+    const int cbits = 2 * shift;
+    ctx->list_shift = shift;
     // M2L
     const int nm = ctx->n_m2l;
     CK(ctx->m2l_seg_b.ensure(nc), "alloc lists");
@@ -591,12 +594,12 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     if (nm > 0) {
         CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
         CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
-        k_expand_m2l<<<grid_for(nm, 256), 256, 0, s>>>(ctx->m2l.p, nm, ctx->m2l_keys.p);
+        k_expand_m2l<<<grid_for(nm, 256), 256, 0, s>>>(ctx->m2l.p, nm, shift, ctx->m2l_keys.p);
         LCOUNT(3);
         size_t tb = sort_keys_u64_temp(2 * nm, cbits);
         CK(ctx->cub_tmp.ensure(tb), "alloc sort");
         CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
-        k_segments<<<grid_for(2 * (size_t)nm, 256), 256, 0, s>>>(ctx->m2l_keys_s.p, 2 * nm, ctx->m2l_seg_b.p,
+        k_segments<<<grid_for(2 * (size_t)nm, 256), 256, 0, s>>>(ctx->m2l_keys_s.p, 2 * nm, shift, ctx->m2l_seg_b.p,
                                                                  ctx->m2l_seg_e.p);
         CKL("m2l lists");
     }
@@ -611,15 +614,15 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     if (np > 0) {
         CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
         CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
-        const uint64_t sentinel = (uint64_t)nc << 32;
+        const uint64_t sentinel = (uint64_t)nc << shift;  // above every valid key, within 2 * shift bits
         LCOUNT(3);
-        k_expand_p2p<<<grid_for(np, 256), 256, 0, s>>>(ctx->p2p.p, np, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
+        k_expand_p2p<<<grid_for(np, 256), 256, 0, s>>>(ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
                                                        ctx->inter.p);
         size_t tb = sort_keys_u64_temp(2 * np, cbits);
         CK(ctx->cub_tmp.ensure(tb), "alloc sort");
         CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->p2p_keys.p, ctx->p2p_keys_s.p, 2 * np, cbits, s), "p2p sort");
         const int nvalid = 2 * np - ctx->nleaves;
-        k_segments<<<grid_for(nvalid, 256), 256, 0, s>>>(ctx->p2p_keys_s.p, nvalid, ctx->p2p_seg_b.p,
+        k_segments<<<grid_for(nvalid, 256), 256, 0, s>>>(ctx->p2p_keys_s.p, nvalid, shift, ctx->p2p_seg_b.p,
                                                          ctx->p2p_seg_e.p);
         CKL("p2p lists");
     }
@@ -760,8 +763,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     }
     if (tm) CK(cudaEventRecord(ev[5], s), "event");
 
-    DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p};
-    DirList lp{ctx->p2p_keys_s.p, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p};
+    DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p, ctx->list_shift};
+    DirList lp{ctx->p2p_keys_s.p, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p, ctx->list_shift};
     if (mixed) {
         fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot);
         if (ms != FMMX_OK) return ms;

@@ -6,23 +6,25 @@
 // mutual pair (a, b) becomes the two directed entries a->b and b->a, a leaf
 // self pair one entry. Entries are radix-sorted by (dst, src), which makes the
 // accumulation order, and therefore every result bit, independent of the
-// order in which the walk's atomics appended pairs.
+// order in which the walk's atomics appended pairs. A key is
+// (dst << shift) | src with shift = the bit width of the cell count, so the
+// sort runs over 2 * shift bits (32 for up to 65535 cells) instead of 64.
 #include "common.cuh"
 #include "kernels.h"
 
 namespace fmmx {
 
-__global__ void k_expand_m2l(const uint2* __restrict__ pairs, int np, uint64_t* __restrict__ keys) {
+__global__ void k_expand_m2l(const uint2* __restrict__ pairs, int np, int shift, uint64_t* __restrict__ keys) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
         const uint2 pr = pairs[q];
-        keys[2 * (size_t)q] = ((uint64_t)pr.y << 32) | pr.x;      // a -> b
-        keys[2 * (size_t)q + 1] = ((uint64_t)pr.x << 32) | pr.y;  // b -> a
+        keys[2 * (size_t)q] = ((uint64_t)pr.y << shift) | pr.x;      // a -> b
+        keys[2 * (size_t)q + 1] = ((uint64_t)pr.x << shift) | pr.y;  // b -> a
     }
 }
 
 // P2P: a self pair gives one entry; its second slot gets `sentinel`, a key
 // above every valid one, so the valid entries are a prefix after sorting.
-__global__ void k_expand_p2p(const uint2* __restrict__ pairs, int np, const uint32_t* __restrict__ count,
+__global__ void k_expand_p2p(const uint2* __restrict__ pairs, int np, int shift, const uint32_t* __restrict__ count,
                              uint64_t sentinel, uint64_t* __restrict__ keys,
                              unsigned long long* __restrict__ interactions) {
     unsigned long long local = 0;
@@ -30,12 +32,12 @@ __global__ void k_expand_p2p(const uint2* __restrict__ pairs, int np, const uint
         const uint2 pr = pairs[q];
         const unsigned long long ca = count[pr.x], cb = count[pr.y];
         if (pr.x == pr.y) {
-            keys[2 * (size_t)q] = ((uint64_t)pr.x << 32) | pr.x;
+            keys[2 * (size_t)q] = ((uint64_t)pr.x << shift) | pr.x;
             keys[2 * (size_t)q + 1] = sentinel;
             local += ca * (ca - 1);
         } else {
-            keys[2 * (size_t)q] = ((uint64_t)pr.y << 32) | pr.x;
-            keys[2 * (size_t)q + 1] = ((uint64_t)pr.x << 32) | pr.y;
+            keys[2 * (size_t)q] = ((uint64_t)pr.y << shift) | pr.x;
+            keys[2 * (size_t)q + 1] = ((uint64_t)pr.x << shift) | pr.y;
             local += 2ull * ca * cb;
         }
     }
@@ -43,12 +45,12 @@ __global__ void k_expand_p2p(const uint2* __restrict__ pairs, int np, const uint
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(interactions, local);
 }
 
-__global__ void k_segments(const uint64_t* __restrict__ keys, int nkeys, uint32_t* __restrict__ seg_begin,
+__global__ void k_segments(const uint64_t* __restrict__ keys, int nkeys, int shift, uint32_t* __restrict__ seg_begin,
                            uint32_t* __restrict__ seg_end) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nkeys; i += gridDim.x * blockDim.x) {
-        const uint32_t d = (uint32_t)(keys[i] >> 32);
-        if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != d) seg_begin[d] = i;
-        if (i == nkeys - 1 || (uint32_t)(keys[i + 1] >> 32) != d) seg_end[d] = i + 1;
+        const uint32_t d = (uint32_t)(keys[i] >> shift);
+        if (i == 0 || (uint32_t)(keys[i - 1] >> shift) != d) seg_begin[d] = i;
+        if (i == nkeys - 1 || (uint32_t)(keys[i + 1] >> shift) != d) seg_end[d] = i + 1;
     }
 }
 
