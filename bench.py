@@ -288,6 +288,15 @@ class _NullCtx:
         return False
 
 
+# DRAM bytes (read + write) per directed M2L translation, from one ncu capture of
+# the M2L launch at N = 262144 (uniform cube, p = 10, theta 0.5, leaf 64: 5,809,554
+# directed translations); the expansions are L2-resident, so the traffic grows
+# with the translation count. See profiles/m2l_rotw_f32_p10_n262144.md and
+# profiles/m2l_rotw_f64_p10_n262144.md.
+M2L_DRAM_BYTES_PER_TRANSLATION = {("mixed", 10): (57.778432e6 + 1.495296e6) / 5809554,
+                                  ("plain", 10): (84.023808e6 + 21.590272e6) / 5809554}
+
+
 def roofline(args, cfg, r, precision, dev):
     import fmms_b200 as fx
 
@@ -297,8 +306,12 @@ def roofline(args, cfg, r, precision, dev):
     fp64 = precision == "plain"
     peak = fx.probe_fma_peak(fp64=fp64, device=dev)
     achieved = fl / (r["m2l_ms"] * 1e-3) / 1e12
+    bpt = M2L_DRAM_BYTES_PER_TRANSLATION.get((precision, cfg["p"])) if kernel == "rotation" else None
+    traffic = bpt * st["m2l_directed"] if bpt is not None else None
     return {"bound": "fp64" if fp64 else "fp32", "kernel": "m2l", "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_note": "DRAM bytes per launch, scaled by directed translations from an ncu capture at "
+                            "N=262144" if traffic is not None else "no capture for this order",
             "peak_source": "measured: FMA loop on every SM (fmmx_probe_fma_peak); MEASURED_PEAKS.json holds only "
                            "HBM and bf16-tensor peaks",
             "algorithmic_flops_per_launch": fl, "launch_ms": r["m2l_ms"],
