@@ -578,6 +578,7 @@ def run_serve(args, cfg, rank, world, local_rank):
                       "admitted_sessions_mean": float(np.mean([o[0] for o in occ])) if occ else 0.0,
                       "admitted_bodies_mean": float(np.mean([o[1] for o in occ])) if occ else 0.0,
                       "lanes": [{"n_from": ln.lo, "stream_priority": ln.priority, "ticks": len(ln.tick_ms),
+                                 "joins_undone": ln.evictions,
                                  "tick_ms_p50": float(np.percentile(ln.tick_ms, 50)) if ln.tick_ms else None}
                                 for ln in srv.lanes],
                       "p99_over_isolated": {"median": float(np.median(rr)) if rr else None,

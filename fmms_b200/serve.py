@@ -29,7 +29,12 @@ predicted with it -- the batch's last measured step latency plus the session's
 calibrated extra latency (the larger of the two system types) -- stays within
 `headroom` times the isolated latency (the smaller of the two types) of the
 batch's smallest session, and only while the lane's recent steps stay within
-that bound (feedback against prediction error). The queue is scanned in arrival
+that bound (feedback against prediction error). The joining tick measures the
+prediction: if it took longer than `headroom` times the isolated latency of the
+batch's smallest session, the sessions that joined in it (all of them when
+others were already stepping, else all but the first) -- which have not
+stepped yet, so nothing of theirs changes -- go back to the front of the queue
+and wait for a session of the lane to finish before they are tried again. The queue is scanned in arrival
 order and sessions that fit may overtake ones that do not, except a session
 that has waited longer than `max_bypass_s`: nobody overtakes it. Waiting time
 is reported apart from the step latency.
@@ -68,7 +73,7 @@ LANE_BOUNDS = (0,)
 CALIBRATION_N = (1_000, 3_000, 10_000, 30_000, 100_000, 300_000, 1_000_000)
 
 
-@dataclasses.dataclass
+@dataclasses.dataclass(eq=False)  # sessions compare by identity
 class Session:
     sid: int
     mass: np.ndarray
@@ -84,6 +89,7 @@ class Session:
     steps_done: int = 0
     primed: bool = False
     last_end: float = 0.0  # end of its last step (or of its joining tick)
+    retry_after: int = -1  # after a failed join: the lane's departure count it must wait past
     step_ms: list = dataclasses.field(default_factory=list)
     result_pos: np.ndarray | None = None
     result_vel: np.ndarray | None = None
@@ -100,8 +106,8 @@ class Session:
     def fresh(self) -> "Session":
         """The same request, not yet served."""
         return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
-                                   primed=False, last_end=0.0, step_ms=[], result_pos=None, result_vel=None,
-                                   staged=None, pending=None)
+                                   primed=False, last_end=0.0, retry_after=-1, step_ms=[], result_pos=None,
+                                   result_vel=None, staged=None, pending=None)
 
 
 def _interp_loglog(ns, vals, n):
@@ -155,6 +161,8 @@ class Lane:
         self.predicted_ms = None  # predicted interval after the last admission, until measured
         self.recent_ratio: deque[float] = deque(maxlen=8)
         self.bodies_stepped = 0
+        self.departures = 0  # sessions finished in this lane
+        self.evictions = 0  # joins undone because the joining tick broke the bound
 
     # ---------------------------------------------------------------- helpers
     @staticmethod
@@ -184,8 +192,8 @@ class Lane:
         nmin = min((s.n for s in self.members), default=None)
         for s in list(self.queue)[: srv.scan]:
             pred = None
-            fits = True
-            if model is not None and nmin is not None:
+            fits = s.retry_after < self.departures
+            if fits and model is not None and nmin is not None:
                 pred = (tau if tau is not None else model.iso(nmin)) + model.extra(s.n)
                 fits = pred <= srv.headroom * model.iso(min(nmin, s.n))
             if fits and srv.reserve(s.bytes_needed()):
@@ -234,6 +242,29 @@ class Lane:
         d = np.concatenate([np.full(s.n, s.dt if s.primed else 0.0) for s in self.members])
         self.dts = torch.from_numpy(d).to(self.srv.dev)[:, None]
 
+    def evict(self, sessions):
+        """Undo the join of sessions that have not stepped: drop their rows and
+        put them back at the front of the queue until a session finishes."""
+        torch = self.srv.torch
+        out = set(id(s) for s in sessions)
+        keep, rows = [], []
+        off = self.offsets(self.members)
+        for i, s in enumerate(self.members):
+            if id(s) not in out:
+                keep.append(s)
+                rows.append(torch.arange(int(off[i]), int(off[i + 1]), device=self.srv.dev))
+        idx = torch.cat(rows)
+        self.state = [t.index_select(0, idx) for t in self.state]
+        self.members = keep
+        for s in reversed(sessions):
+            s.admitted_at = None
+            s.retry_after = self.departures
+            self.srv.release(s.bytes_needed())
+            self.queue.appendleft(s)
+        self.evictions += len(sessions)
+        self.predicted_ms = None
+        self._set_dts()
+
     def leave(self, now):
         torch = self.srv.torch
         keep, rows, out = [], [], []
@@ -246,6 +277,7 @@ class Lane:
             else:
                 keep.append(s)
                 rows.append(torch.arange(a, b, device=self.srv.dev))
+        self.departures += len(out)
         for s, p, v in out:
             ev = torch.cuda.Event()
             ev.record(self.stream)
@@ -270,6 +302,7 @@ class Lane:
     # ---------------------------------------------------------------- one tick
     def tick(self) -> float:
         torch = self.srv.torch
+        t_start = time.perf_counter()
         with torch.cuda.stream(self.stream):
             self.join(self.admit(time.perf_counter()))
             if not self.members:
@@ -301,6 +334,13 @@ class Lane:
                 if self.srv.model is not None:
                     self.recent_ratio.append(max(s.step_ms[-1] / self.srv.model.iso(s.n) for s in stepping))
             joined = [s for s in self.members if not s.primed]
+            model = self.srv.model
+            if joined and model is not None and len(self.members) > 1:
+                ratio = 1e3 * (t_end - t_start) / model.iso(min(s.n for s in self.members))
+                undo = joined if stepping else joined[1:]
+                if ratio > self.srv.headroom and undo:
+                    self.evict(undo)
+                    joined = [s for s in joined if s not in undo]
             for s in joined:
                 s.primed = True
                 s.last_end = t_end
