@@ -435,6 +435,82 @@ def run_kdk(args, cfg, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ C3: same-error comparison
+# (p, theta, soft_gap): soft_gap > 0 keeps M2L pairs soft_gap * softening apart
+SWEEP_SETTINGS = ((12, 0.4, 0.0), (16, 0.4, 0.0), (12, 0.3, 0.0), (12, 0.4, 100.0), (12, 0.4, 300.0),
+                  (10, 0.5, 100.0), (10, 0.5, 200.0), (10, 0.5, 300.0), (8, 0.5, 300.0), (8, 0.4, 300.0),
+                  (10, 0.6, 300.0), (12, 0.5, 300.0))
+
+
+def run_accuracy_sweep(args, cfg, rank, world, local_rank):
+    """The clustered workload's force evaluation at several (p, theta) in both
+    precisions: bodies/s and p99 relative error against the FP64 direct sum
+    on 4096 seeded targets; then, per precision, the fastest setting whose p99
+    error is <= 1e-5, and the ratio of the two (mixed over plain at the same
+    error bound)."""
+    import torch
+
+    import fmms_b200 as fx
+
+    if rank != 0:
+        return
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    mass, pos, _ = fx.gen_clusters(cfg["n"], 64, 1e-3, 1e-1, SEEDS["clusters"])
+    n = len(mass)
+    tg = np.sort(np.random.default_rng(4096).choice(n, size=4096, replace=False)).astype(np.uint32)
+    a_ref, _, _ = fx.direct_targets(mass, pos, tg, softening=cfg["softening"], device=dev)
+    d_pos = torch.from_numpy(pos).to(f"cuda:{dev}")
+    d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+    d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    rows = []
+    for prec in ("mixed", "plain"):
+        for p, theta, gap in SWEEP_SETTINGS:
+            g = fx.Fmm(None, None, p, 0.0, cfg["n_leaf"], mac="theta", theta=theta, softening=cfg["softening"],
+                       precision=prec, device=dev, stream=stream.cuda_stream, soft_gap=gap)
+            ms = []
+            for it in range(3):  # one warm-up, two timed
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+                g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+                e1.record(stream)
+                e1.synchronize()
+                if it:
+                    ms.append(e0.elapsed_time(e1))
+            a = d_acc.cpu().numpy()[tg]
+            rel = np.linalg.norm(a - a_ref, axis=1) / np.linalg.norm(a_ref, axis=1)
+            st = g.stats()
+            g.close()
+            rows.append({"precision": prec, "p": p, "theta": theta, "soft_gap": gap, "ms": float(np.mean(ms)),
+                         "bodies_per_s": n / (np.mean(ms) * 1e-3), "err_p50": float(np.percentile(rel, 50)),
+                         "err_p99": float(np.percentile(rel, 99)), "m2l_ms": st["ms_m2l"], "p2p_ms": st["ms_p2p"],
+                         "n_m2l": int(st["n_m2l"]), "p2p_interactions": int(st["p2p_interactions"])})
+            print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    best = {}
+    for prec in ("mixed", "plain"):
+        ok = [r for r in rows if r["precision"] == prec and r["err_p99"] <= 1e-5]
+        best[prec] = max(ok, key=lambda r: r["bodies_per_s"]) if ok else None
+    ratio = (best["mixed"]["bodies_per_s"] / best["plain"]["bodies_per_s"]
+             if best["mixed"] and best["plain"] else None)
+    main = best["mixed"] or max((r for r in rows if r["precision"] == "mixed"), key=lambda r: -r["err_p99"])
+    line = {"metric": METRIC, "value": main["bodies_per_s"], "unit": "bodies/s", "n_gpus": 1, "steps": 2,
+            "warmup": 1, "ms_per_step": main["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "dtype": "f32+f64",
+            "config": {"workload": cfg["workload"].split(", p=")[0] + ", one force evaluation per setting",
+                       "settings_p_theta_softgap": [list(t) for t in SWEEP_SETTINGS], "n_leaf": cfg["n_leaf"],
+                       "l2": "flushed between timed evaluations"},
+            "same_error": {"bound_p99": 1e-5, "mixed": best["mixed"], "plain": best["plain"],
+                           "mixed_over_plain": ratio},
+            "sweep": rows}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ C4: ensemble
 def run_ensemble(args, cfg, rank, world, local_rank):
     """512 independent Plummer spheres (N log-uniform in [1e3, 1e5], scale
@@ -611,6 +687,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override N (small cases for profiling)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="c3: force evaluations at several (p, theta) in both precisions, compared at p99 <= 1e-5")
     args = ap.parse_args()
     cfg = dict(CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config])
     if args.n > 0:
@@ -631,7 +709,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        runner = {"c3": run_kdk, "c4": run_ensemble, "c5": run_serve}.get(args.config, run_gpu)
+        runner = {"c3": run_accuracy_sweep if args.sweep else run_kdk, "c4": run_ensemble,
+                  "c5": run_serve}.get(args.config, run_gpu)
         runner(args, cfg, rank, world, local_rank)
     finally:
         if world > 1:

@@ -67,6 +67,7 @@ class Config(C.Structure):
         ("stream", C.c_void_p),
         ("p2p_tile", C.c_int),
         ("preemptible", C.c_int),
+        ("soft_gap", C.c_double),
     ]
 
 
@@ -180,13 +181,14 @@ class Fmm:
     ``Fmm(mass, pos, p, eps, n_leaf)`` builds the tree like ``Fmm::new``. The
     keyword arguments select the extensions: ``mac='theta'`` with ``theta``,
     ``softening``, ``precision='mixed'``, ``center='sphere'`` (as
-    ``Fmm::with_center``), ``m2l='naive'|'rotation'``.
+    ``Fmm::with_center``), ``m2l='naive'|'rotation'``, ``soft_gap`` (M2L only
+    between cells whose bodies are soft_gap * softening apart).
     """
 
     def __init__(self, mass, pos, p: int = 8, eps: float = 1e-5, n_leaf: int = 16, *, mac: str = "dehnen",
                  theta: float = 0.5, softening: float = 0.0, precision: str = "plain", center: str = "com",
                  m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0,
-                 preemptible: bool = False):
+                 preemptible: bool = False, soft_gap: float = 0.0):
         cfg = Config()
         lib().fmmx_config_default(C.byref(cfg))
         cfg.p = int(p)
@@ -202,6 +204,7 @@ class Fmm:
         cfg.stream = stream
         cfg.p2p_tile = int(p2p_tile)
         cfg.preemptible = 1 if preemptible else 0
+        cfg.soft_gap = float(soft_gap)
         self.cfg = cfg
         self.p = cfg.p
         h = _vp()

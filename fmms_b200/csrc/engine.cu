@@ -521,6 +521,7 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
     mp.p = ctx->cfg.p;
     mp.eps = ctx->cfg.mac_eps;
     mp.theta = ctx->cfg.theta;
+    mp.gap = ctx->cfg.soft_gap * ctx->cfg.softening;
     const CellsView cv = view(ctx);
     for (int attempt = 0;; ++attempt) {
         CK(ctx->front0.ensure(ctx->cap_front), "alloc walk");
@@ -859,6 +860,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->stream = nullptr;
     c->p2p_tile = 0;
     c->preemptible = 0;
+    c->soft_gap = 0.0;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -891,6 +893,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (c.precision != FMMX_PLAIN_FP64 && c.precision != FMMX_MIXED) return FMMX_INVALID_ARG;
     if (c.p2p_tile < 0 || c.p2p_tile > 512) return FMMX_INVALID_ARG;
     if (c.preemptible != 0 && c.preemptible != 1) return FMMX_INVALID_ARG;
+    if (!(c.soft_gap >= 0.0) || !std::isfinite(c.soft_gap)) return FMMX_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

@@ -38,6 +38,7 @@ struct MacParams {
     int p;
     double eps;
     double theta;
+    double gap;  // minimum separation of the bodies of an M2L pair (soft_gap * softening); 0: none
 };
 
 enum { WC_FRONT0 = 0, WC_FRONT1 = 1, WC_M2L = 2, WC_P2P = 3, WC_OVERFLOW = 4, WC_SIZE = 8 };

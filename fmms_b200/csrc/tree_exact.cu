@@ -749,6 +749,15 @@ __device__ __forceinline__ bool accept_theta(const CellsView& cv, const MacParam
     return sum_rho < mp.theta * sqrt(r2);
 }
 
+// Separation condition (extension, with softening): the bodies of the two
+// cells are at least mp.gap apart, r - rho_A - rho_B >= gap.
+__device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp, int a, int b) {
+    if (!(mp.gap > 0.0)) return true;
+    const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    return sqrt(r2) - (cv.rho[a] + cv.rho[b]) >= mp.gap;
+}
+
 // ------------------------------------------------------------ dual walk
 // process_pair, walk.rs:94-190, applied to a whole frontier of cell pairs at
 // once. Every decision depends only on the pair, so the emitted M2L and P2P
@@ -800,6 +809,7 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
             acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a);
         else
             acc = accept_theta(cv, mp, a, b) && accept_theta(cv, mp, b, a);
+        acc = acc && gap_ok(cv, mp, a, b);
         if (acc) {
             int s = atomicAdd(&w.counts[WC_M2L], 1);
             if ((uint32_t)s < w.cap_m2l) w.m2l[s] = make_uint2(a, b);

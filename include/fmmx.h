@@ -75,6 +75,10 @@ typedef struct fmmx_config {
     int preemptible;   /* 1: the M2L runs one short block per destination cell instead of persistent warps,
                           so kernels on higher-priority streams start between its blocks (serving lanes);
                           0 (default): persistent warps, the faster form for one evaluation at a time */
+    double soft_gap;   /* extension, with softening > 0: a cell pair is accepted for M2L only if its bodies are
+                          at least soft_gap * softening apart (r - rho_A - rho_B), on top of the MAC. The far
+                          field uses the unsoftened kernel, which errs by about softening^2 / (2 d^2) relative
+                          at distance d; this bounds that error. 0 (default): no such condition */
 } fmmx_config;
 
 typedef struct fmmx_stats {

@@ -59,6 +59,7 @@ def lib():
         L.orc_fmm_new.restype = C.c_void_p
         L.orc_fmm_refresh.argtypes = [C.c_void_p, _sz, _dp, _dp]
         L.orc_fmm_free.argtypes = [C.c_void_p]
+        L.orc_fmm_set_gap.argtypes = [C.c_void_p, C.c_double]
         L.orc_fmm_run.argtypes = [C.c_void_p, _sz, _dp, _dp, C.c_int, _dp, _dp]
         L.orc_fmm_ncells.argtypes = [C.c_void_p]
         L.orc_fmm_ncells.restype = _sz
@@ -240,7 +241,8 @@ MAC_THETA = 1
 class Fmm:
     """Mirror of fmm::Fmm (fmm.rs:10-142) over the oracle."""
 
-    def __init__(self, mass, pos, p, eps, n_leaf, *, mac=MAC_DEHNEN, theta=0.5, softening=0.0, center=0):
+    def __init__(self, mass, pos, p, eps, n_leaf, *, mac=MAC_DEHNEN, theta=0.5, softening=0.0, center=0,
+                 soft_gap=0.0):
         self.mass = np.ascontiguousarray(mass, dtype=np.float64)
         self.pos = np.ascontiguousarray(pos, dtype=np.float64)
         self.n = len(self.mass)
@@ -249,6 +251,8 @@ class Fmm:
                                     softening, n_leaf, center)
         if not self._h:
             raise ValueError("empty input")
+        if soft_gap:
+            lib().orc_fmm_set_gap(self._h, soft_gap * softening)
 
     def __del__(self):
         h = getattr(self, "_h", None)

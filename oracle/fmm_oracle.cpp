@@ -515,6 +515,7 @@ struct MacCtx {
     int mode;
     double eps;    // Dehnen accuracy parameter (reference `eps`)
     double theta;  // geometric opening angle (extension)
+    double gap;    // minimum separation of an M2L pair's bodies (extension, with softening); 0: none
     size_t p;
     const std::vector<Cell>* cells;
     const double* pows;
@@ -565,6 +566,18 @@ static bool accept_theta(const MacCtx& mc, size_t ai, size_t bi) {
     double sum_rho = ca.rho + cb.rho;
     double r = std::sqrt(r2);
     return sum_rho < mc.theta * r;
+}
+
+// Separation condition (extension): r - rho_A - rho_B >= gap.
+static bool gap_ok(const MacCtx& mc, size_t ai, size_t bi) {
+    if (!(mc.gap > 0.0)) return true;
+    const Cell& ca = (*mc.cells)[ai];
+    const Cell& cb = (*mc.cells)[bi];
+    double dx = cb.cen[0] - ca.cen[0];
+    double dy = cb.cen[1] - ca.cen[1];
+    double dz = cb.cen[2] - ca.cen[2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    return std::sqrt(r2) - (ca.rho + cb.rho) >= mc.gap;
 }
 
 static inline bool accept(const MacCtx& mc, size_t a, size_t b) {
@@ -1073,7 +1086,7 @@ static void dual_walk(Bodies& b, const Tree& t, const MacCtx& mc, const Cx* mome
                         if (ca.children[j] >= 0) stack.push_back({(size_t)ca.children[i], (size_t)ca.children[j]});
                 }
             }
-        } else if (accept(mc, a, bb) && accept(mc, bb, a)) {
+        } else if (accept(mc, a, bb) && accept(mc, bb, a) && gap_ok(mc, a, bb)) {
             out.m2l.push_back((uint32_t)a);
             out.m2l.push_back((uint32_t)bb);
             if (evaluate) {
@@ -1172,7 +1185,7 @@ struct Fmm {
     Tree tree;
     size_t p;
     MacCtx mc;
-    double mac_eps, theta, soft2;
+    double mac_eps, theta, soft2, gap = 0.0;
     int mac_mode;
     // retained intermediates of the last run (for parity checks)
     size_t n = 0;
@@ -1231,6 +1244,7 @@ static void run(Fmm& F, size_t n, const double* pos, const double* mass, int nth
     F.mc.mode = F.mac_mode;
     F.mc.eps = F.mac_eps;
     F.mc.theta = F.theta;
+    F.mc.gap = F.gap;
     F.mc.p = p;
     F.mc.cells = &t.cells;
     F.mc.pows = F.pows.data();
@@ -1409,6 +1423,8 @@ void orc_fmm_refresh(void* h, size_t n, const double* pos, const double* mass) {
     build_tree(F->tree, n, pos, mass, F->tree.n_leaf, F->tree.mode);
 }
 void orc_fmm_free(void* h) { delete (Fmm*)h; }
+// Separation condition of the M2L pairs (extension): absolute gap, 0 = none.
+void orc_fmm_set_gap(void* h, double gap) { ((Fmm*)h)->gap = gap; }
 void orc_fmm_run(void* h, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot) {
     run(*(Fmm*)h, n, pos, mass, nthreads, acc, pot);
 }

@@ -40,6 +40,8 @@ def check_case(orc, mass, pos, p, eps, n_leaf, *, acc_tol=ACC_TOL, loc_tol=1e-11
         okw["softening"] = kw["softening"]
     if kw.get("center") == "sphere":
         okw["center"] = 1
+    if "soft_gap" in kw:
+        okw["soft_gap"] = kw["soft_gap"]
     g = fx().Fmm(mass, pos, p, eps, n_leaf, **kw)
     res = g.run()
     o = orc.Fmm(mass, pos, p, eps, n_leaf, **okw)
@@ -92,6 +94,19 @@ def test_hernquist(orc):
 def test_theta_mac_softened(orc):
     mass, pos = orc.plummer(16384, seed=99)
     check_case(orc, mass, pos, 8, 0.0, 64, mac="theta", theta=0.5, softening=1e-3)
+
+
+@pytest.mark.parametrize("mac", ["theta", "dehnen"])
+def test_softening_gap(orc, mac):
+    """M2L only between cells whose bodies are soft_gap * softening apart
+    (extension): the same pair sets as the oracle, forces to 1e-12."""
+    mass, pos = orc.plummer(16384, seed=7)
+    kw = dict(mac="theta", theta=0.5) if mac == "theta" else {}
+    g, _ = check_case(orc, mass, pos, 8, 1e-6, 32, softening=0.02, soft_gap=10.0, **kw)
+    m2l_g, _ = g.export_lists()
+    h, _ = check_case(orc, mass, pos, 8, 1e-6, 32, softening=0.02, **kw)
+    m2l_h, _ = h.export_lists()
+    assert len(m2l_g) < len(m2l_h)  # the condition removed pairs
 
 
 def test_rotation_m2l(orc):
