@@ -718,11 +718,10 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     }
     if (mixed && !dehnen) {
         // normalised FP32 upward pass; FP64 accumulation on the top three levels
-        const int warps = 4;
         for (int L = ctx->nlevels - 1; L >= 0; --L) {
             const int cnt = ctx->lvl_count[L];
-            const unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, kGrid);
-            launch_upward_mixed(L <= 2, g, warps, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->ell.p,
+            const unsigned g = std::min<unsigned>(cnt, 148u * 16u);
+            launch_upward_mixed(L <= 2, g, 4, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->ell.p,
                                 ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->mom_f.p);
         }
         CKL("upward (mixed)");

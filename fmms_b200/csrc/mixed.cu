@@ -88,92 +88,92 @@ __global__ void k_moments_to_mixed(int nc, int p, const zd* __restrict__ full, c
     }
 }
 
-// P2M / M2M for one level, one warp per cell. A = accumulation type (double
-// on the top three levels, float below). Output FP32 half layout.
+// P2M / M2M for one level, one 128-thread CTA per cell. A = accumulation type
+// (double on the top three levels, float below). Output FP32 half layout.
+//  - leaf (P2M): thread t takes column m = t % (p+1) of the bodies
+//    g, g+G, g+2G, ... (g = t / (p+1), G <= 8 groups), accumulating the column
+//    in its own shared-memory entries; the group partials are then summed in a
+//    fixed order;
+//  - internal (M2M): first the Υ tables of the eight child offsets (one thread
+//    per child and column), then one thread per (child, entry) computes that
+//    child's contribution, and the children are summed in octant order.
+#define UPM_BLOCK 128
 template <typename A>
-__global__ void k_upward_mixed(const int32_t* __restrict__ level_cells, int lstart, int lcnt, CellsView cv,
-                               const double* __restrict__ ell, const double* __restrict__ x,
-                               const double* __restrict__ y, const double* __restrict__ z,
-                               const double* __restrict__ m, int p, zf* __restrict__ mom) {
+__global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __restrict__ level_cells, int lstart,
+                                                            int lcnt, CellsView cv, const double* __restrict__ ell,
+                                                            const double* __restrict__ x,
+                                                            const double* __restrict__ y,
+                                                            const double* __restrict__ z,
+                                                            const double* __restrict__ m, int p,
+                                                            zf* __restrict__ mom) {
     extern __shared__ unsigned char smem_raw[];
     const int H = (p + 1) * (p + 2) / 2;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw) + (size_t)wib * 2 * H;
-    cplx<A>* acc = u + H;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int j = warp; j < lcnt; j += nwarps) {
+    const int P1 = p + 1;
+    cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw);  // 8 x H: Υ of the child offsets
+    cplx<A>* part = u + 8 * H;                          // 8 x H: partial sums
+    const int tid = threadIdx.x;
+    const int G = min(8, UPM_BLOCK / P1);
+    for (int j = blockIdx.x; j < lcnt; j += gridDim.x) {
         const int c = level_cells[lstart + j];
         const double sx = cv.cx[c], sy = cv.cy[c], sz = cv.cz[c];
         const double il = 1.0 / ell[c];
-        for (int e = lane; e < H; e += 32) acc[e] = mk<A>(A(0), A(0));
-        __syncwarp();
+        int nparts;
         if (cv.leaf[c]) {
-            // lanes over bodies, each with its own Υ table column set: lane
-            // handles body b, all columns; sums into acc by warp reduction per entry
-            const uint32_t f = cv.first[c], cnt = cv.count[c];
-            for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
-                const uint32_t b = b0 + lane;
-                const bool act = b < cnt;
-                A rx = 0, ry = 0, rz = 0, mb = 0;
-                if (act) {
-                    rx = (A)((x[f + b] - sx) * il);
-                    ry = (A)((y[f + b] - sy) * il);
-                    rz = (A)((z[f + b] - sz) * il);
-                    mb = (A)m[f + b];
-                }
-                const A r2 = rx * rx + ry * ry + rz * rz;
-                cplx<A> d = mk<A>(A(1), A(0));
-                for (int mm = 0; mm <= p; ++mm) {
-                    if (mm > 0) d = zmul(zscale(mk<A>(rx, ry), (A)c_tab.inv2m[mm]), d);
+            nparts = G;
+            const int mc = tid % P1, g = tid / P1;
+            if (g < G) {
+                cplx<A>* acc = part + g * H;  // this thread's entries hx(n, mc), n >= mc
+                for (int n = mc; n <= p; ++n) acc[hx(n, mc)] = mk<A>(A(0), A(0));
+                const uint32_t f = cv.first[c], cnt = cv.count[c];
+                for (uint32_t b = g; b < cnt; b += G) {
+                    const A rx = (A)((x[f + b] - sx) * il), ry = (A)((y[f + b] - sy) * il),
+                            rz = (A)((z[f + b] - sz) * il);
+                    const A mb = (A)m[f + b];
+                    const A r2 = rx * rx + ry * ry + rz * rz;
+                    cplx<A> d = mk<A>(A(1), A(0));
+                    for (int q = 1; q <= mc; ++q) d = zmul(zscale(mk<A>(rx, ry), (A)c_tab.inv2m[q]), d);
                     cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
-                    for (int n = mm; n <= p; ++n) {
-                        cplx<A> un;
-                        if (n == mm) {
-                            un = d;
-                        } else {
-                            const A a = (A)(2 * n - 1) * rz;
-                            un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][mm]);
-                            u2 = u1;
-                            u1 = un;
-                        }
-                        A vr = un.re * mb, vi = un.im * mb;
-                        for (int o = 16; o > 0; o >>= 1) {
-                            vr += __shfl_xor_sync(0xffffffffu, vr, o);
-                            vi += __shfl_xor_sync(0xffffffffu, vi, o);
-                        }
-                        if (lane == 0) {
-                            acc[hx(n, mm)].re += vr;
-                            acc[hx(n, mm)].im += vi;
-                        }
+                    acc[hx(mc, mc)].re += d.re * mb;
+                    acc[hx(mc, mc)].im += d.im * mb;
+                    for (int n = mc + 1; n <= p; ++n) {
+                        const A a = (A)(2 * n - 1) * rz;
+                        const cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][mc]);
+                        u2 = u1;
+                        u1 = un;
+                        acc[hx(n, mc)].re += un.re * mb;
+                        acc[hx(n, mc)].im += un.im * mb;
                     }
                 }
-                __syncwarp();
             }
         } else {
-            for (int o = 0; o < 8; ++o) {
+            nparts = 8;
+            for (int w = tid; w < 8 * P1; w += UPM_BLOCK) {
+                const int o = w / P1, mc = w % P1;
                 const int ch = cv.child[8 * c + o];
                 if (ch < 0) continue;
                 const A dx = (A)((cv.cx[ch] - sx) * il), dy = (A)((cv.cy[ch] - sy) * il),
                         dz = (A)((cv.cz[ch] - sz) * il);
-                const A r2 = dx * dx + dy * dy + dz * dz;
-                for (int mm = lane; mm <= p; mm += 32) ups_column<A>(dx, dy, dz, r2, p, mm, u);
-                __syncwarp();
-                const A ratio = (A)(ell[ch] * il);
-                const zf* mc = mom + (size_t)ch * H;
-                for (int e = lane; e < H; e += 32) {
+                ups_column<A>(dx, dy, dz, dx * dx + dy * dy + dz * dz, p, mc, u + o * H);
+            }
+            __syncthreads();
+            for (int w = tid; w < 8 * H; w += UPM_BLOCK) {
+                const int o = w / H, e = w % H;
+                const int ch = cv.child[8 * c + o];
+                A sr = 0, si = 0;
+                if (ch >= 0) {
                     int n, mm;
                     split_h(e, n, mm);
-                    A sr = 0, si = 0;
+                    const cplx<A>* uo = u + o * H;
+                    const A ratio = (A)(ell[ch] * il);
+                    const zf* mcv = mom + (size_t)ch * H;
                     A rpow = 1;  // ratio^{n-k}, built from k = n down
                     for (int k = n; k >= 0; --k) {
                         const int nk = n - k;
                         const int lo = max(-k, mm - nk), hi = min(k, mm + nk);
                         A tr = 0, ti = 0;
                         for (int l = lo; l <= hi; ++l) {
-                            const cplx<A> uu = half_get<A>(u, k, l);
-                            const zf mv = half_get<float>(mc, nk, mm - l);
+                            const cplx<A> uu = half_get<A>(uo, k, l);
+                            const zf mv = half_get<float>(mcv, nk, mm - l);
                             tr += uu.re * (A)mv.re - uu.im * (A)mv.im;
                             ti += uu.re * (A)mv.im + uu.im * (A)mv.re;
                         }
@@ -181,28 +181,35 @@ __global__ void k_upward_mixed(const int32_t* __restrict__ level_cells, int lsta
                         si += ti * rpow;
                         rpow *= ratio;
                     }
-                    acc[e].re += sr;
-                    acc[e].im += si;
                 }
-                __syncwarp();
+                part[o * H + e] = mk<A>(sr, si);
             }
         }
+        __syncthreads();
         zf* out = mom + (size_t)c * H;
-        for (int e = lane; e < H; e += 32) out[e] = mk<float>((float)acc[e].re, (float)acc[e].im);
-        __syncwarp();
+        for (int e = tid; e < H; e += UPM_BLOCK) {
+            A sr = 0, si = 0;
+            for (int q = 0; q < nparts; ++q) {
+                sr += part[q * H + e].re;
+                si += part[q * H + e].im;
+            }
+            out[e] = mk<float>((float)sr, (float)si);
+        }
+        __syncthreads();
     }
 }
 
 void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
                          int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,
                          const double* z, const double* m, int p, zf* mom) {
+    (void)warps;
     const int H = (p + 1) * (p + 2) / 2;
     if (fp64)
-        k_upward_mixed<double><<<grid, 32 * warps, (size_t)warps * 2 * H * sizeof(zd), s>>>(
-            level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+        k_upward_mixed<double><<<grid, UPM_BLOCK, (size_t)16 * H * sizeof(zd), s>>>(level_cells, lstart, lcnt, cv,
+                                                                                    ell, x, y, z, m, p, mom);
     else
-        k_upward_mixed<float><<<grid, 32 * warps, (size_t)warps * 2 * H * sizeof(zf), s>>>(
-            level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+        k_upward_mixed<float><<<grid, UPM_BLOCK, (size_t)16 * H * sizeof(zf), s>>>(level_cells, lstart, lcnt, cv,
+                                                                                   ell, x, y, z, m, p, mom);
 }
 
 // L2L for the cells of one level (L >= 1), one CTA per cell; A as above.

@@ -59,15 +59,24 @@ __global__ void k_bbox_partial(const double* __restrict__ pos, size_t n, double*
 }
 
 // box = {lo[3], hi[3], side, inv_side}; side as tree.rs:107-111.
+// One warp: lanes reduce strided partials, then a shuffle reduction (min and
+// max are exact, so the order does not matter).
 __global__ void k_bbox_final(const double* __restrict__ part, int nparts, double* __restrict__ box) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
     double lo[3] = {INFINITY, INFINITY, INFINITY};
     double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (int b = 0; b < nparts; ++b)
+    for (int b = lane; b < nparts; b += 32)
         for (int d = 0; d < 3; ++d) {
             lo[d] = fmin(lo[d], part[b * 6 + d]);
             hi[d] = fmax(hi[d], part[b * 6 + 3 + d]);
         }
+    for (int o = 16; o > 0; o >>= 1)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+            hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        }
+    if (lane != 0) return;
     double side = fmax(fmax(fmax(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]), DBL_MIN);
     for (int d = 0; d < 3; ++d) {
         box[d] = lo[d];
