@@ -770,14 +770,20 @@ __device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp,
 // ------------------------------------------------------------ dual walk
 // process_pair, walk.rs:94-190, applied to a whole frontier of cell pairs at
 // once. Every decision depends only on the pair, so the emitted M2L and P2P
-// pair sets equal those of the reference's depth-first stack walk.
-__device__ __forceinline__ int push_block(WalkBufs& w, int nxt, int k) {
-    int base = atomicAdd(&w.counts[nxt], k);
-    if ((uint32_t)(base + k) > w.cap_front) {
-        atomicOr(&w.counts[WC_OVERFLOW], 1);
-        return -1;
-    }
-    return base;
+// pair sets equal those of the reference's depth-first stack walk. Appends are
+// warp-aggregated: one atomic per warp and list (a ballot for the M2L and P2P
+// lists, a prefix sum of the child-pair counts for the next frontier); the
+// order within a list is arbitrary, the directed lists are sorted afterwards.
+enum { WK_NONE = 0, WK_M2L = 1, WK_P2P = 2, WK_SPLIT_SELF = 3, WK_SPLIT = 4 };
+
+__device__ __forceinline__ int warp_append(int* counter, bool mine, int lane) {
+    const unsigned mask = __ballot_sync(0xffffffffu, mine);
+    if (!mask) return -1;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return mine ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
 }
 
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict__ pows,
@@ -790,55 +796,85 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.pops_ptr, (unsigned long long)nin);
     const uint2* __restrict__ fin = w.front[cur];
     uint2* fout = w.front[nxt];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nin; q += gridDim.x * blockDim.x) {
-        const uint2 pr = fin[q];
-        const int a = (int)pr.x, b = (int)pr.y;
-        const bool la = cv.leaf[a], lb = cv.leaf[b];
-        if (a == b) {
-            if (la) {
-                int s = atomicAdd(&w.counts[WC_P2P], 1);
-                if ((uint32_t)s < w.cap_p2p) w.p2p[s] = make_uint2(a, a);
-                else atomicOr(&w.counts[WC_OVERFLOW], 2);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    // whole warps step through the frontier together (the ballots need every lane)
+    for (int q0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < nin; q0 += stride) {
+        const int q = q0 + lane;
+        int kind = WK_NONE, a = 0, b = 0, sc = 0, npush = 0;
+        bool split_a = false;
+        if (q < nin) {
+            const uint2 pr = fin[q];
+            a = (int)pr.x;
+            b = (int)pr.y;
+            const bool la = cv.leaf[a], lb = cv.leaf[b];
+            if (a == b) {
+                if (la) {
+                    kind = WK_P2P;
+                } else {
+                    kind = WK_SPLIT_SELF;
+                    sc = a;
+                    int nc = 0;
+                    for (int o = 0; o < 8; ++o) nc += cv.child[8 * a + o] >= 0;
+                    npush = nc * (nc + 1) / 2;
+                }
             } else {
-                const int32_t* ch = cv.child + 8 * a;
-                int nc = 0;
-                for (int o = 0; o < 8; ++o) nc += ch[o] >= 0;
-                int base = push_block(w, nxt, nc * (nc + 1) / 2);
-                if (base < 0) continue;
-                for (int i = 0; i < 8; ++i) {
-                    if (ch[i] < 0) continue;
-                    for (int j = i; j < 8; ++j)
-                        if (ch[j] >= 0) fout[base++] = make_uint2(ch[i], ch[j]);
+                bool acc;
+                if (mp.mode == FMMX_MAC_DEHNEN)
+                    acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a);
+                else
+                    acc = accept_theta(cv, mp, a, b) && accept_theta(cv, mp, b, a);
+                acc = acc && gap_ok(cv, mp, a, b);
+                if (acc) {
+                    kind = WK_M2L;
+                } else if (la && lb) {
+                    kind = WK_P2P;
+                } else {
+                    // split b when a is a leaf or b is the larger cell, else split a
+                    kind = WK_SPLIT;
+                    split_a = lb || (!la && cv.rho[a] >= cv.rho[b]);
+                    sc = split_a ? a : b;
+                    for (int o = 0; o < 8; ++o) npush += cv.child[8 * sc + o] >= 0;
                 }
             }
+        }
+        const int sm = warp_append(&w.counts[WC_M2L], kind == WK_M2L, lane);
+        if (kind == WK_M2L) {
+            if ((uint32_t)sm < w.cap_m2l) w.m2l[sm] = make_uint2(a, b);
+            else atomicOr(&w.counts[WC_OVERFLOW], 4);
+        }
+        const int sp = warp_append(&w.counts[WC_P2P], kind == WK_P2P, lane);
+        if (kind == WK_P2P) {
+            if ((uint32_t)sp < w.cap_p2p) w.p2p[sp] = make_uint2(a, b);
+            else atomicOr(&w.counts[WC_OVERFLOW], 2);
+        }
+        // next frontier: inclusive prefix sum of the pushes across the warp
+        int incl = npush;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total == 0) continue;
+        int base = 0;
+        if (lane == 31) base = atomicAdd(&w.counts[nxt], total);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        if ((uint32_t)(base + total) > w.cap_front) {
+            if (lane == 0) atomicOr(&w.counts[WC_OVERFLOW], 1);
             continue;
         }
-        bool acc;
-        if (mp.mode == FMMX_MAC_DEHNEN)
-            acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a);
-        else
-            acc = accept_theta(cv, mp, a, b) && accept_theta(cv, mp, b, a);
-        acc = acc && gap_ok(cv, mp, a, b);
-        if (acc) {
-            int s = atomicAdd(&w.counts[WC_M2L], 1);
-            if ((uint32_t)s < w.cap_m2l) w.m2l[s] = make_uint2(a, b);
-            else atomicOr(&w.counts[WC_OVERFLOW], 4);
-        } else if (la && lb) {
-            int s = atomicAdd(&w.counts[WC_P2P], 1);
-            if ((uint32_t)s < w.cap_p2p) w.p2p[s] = make_uint2(a, b);
-            else atomicOr(&w.counts[WC_OVERFLOW], 2);
-        } else {
-            // split b when a is a leaf or b is the larger cell, else split a
-            const bool split_a = lb || (!la && cv.rho[a] >= cv.rho[b]);
-            const int sc = split_a ? a : b;
-            const int32_t* ch = cv.child + 8 * sc;
-            int nc = 0;
-            for (int o = 0; o < 8; ++o) nc += ch[o] >= 0;
-            int base = push_block(w, nxt, nc);
-            if (base < 0) continue;
+        int pos = base + incl - npush;
+        const int32_t* ch = cv.child + 8 * sc;
+        if (kind == WK_SPLIT_SELF) {
+            for (int i = 0; i < 8; ++i) {
+                if (ch[i] < 0) continue;
+                for (int j = i; j < 8; ++j)
+                    if (ch[j] >= 0) fout[pos++] = make_uint2(ch[i], ch[j]);
+            }
+        } else if (kind == WK_SPLIT) {
             for (int o = 0; o < 8; ++o) {
                 if (ch[o] < 0) continue;
-                fout[base++] = split_a ? make_uint2(ch[o], b) : make_uint2(a, ch[o]);
+                fout[pos++] = split_a ? make_uint2(ch[o], b) : make_uint2(a, ch[o]);
             }
         }
     }
