@@ -435,6 +435,61 @@ def run_kdk(args, cfg, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ graphs on a reused tree
+def run_graphs(args, cfg, rank, world, local_rank):
+    """Device leapfrog on the given configuration with tree reuse
+    (refresh_every, default 8): steps launched one by one against steps
+    replayed from a CUDA graph, same inputs, mixed precision."""
+    import torch
+
+    import fmms_b200 as fx
+
+    if rank != 0:
+        return
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    mass, pos = make_inputs(fx, cfg)
+    n = len(mass)
+    vel = np.zeros_like(pos)
+    refresh = max(args.refresh_every, 2)
+    res = {}
+    side = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(side):
+        for graphs in (False, True):
+            d_pos = torch.from_numpy(pos.copy()).to(f"cuda:{dev}")
+            d_vel = torch.from_numpy(vel.copy()).to(f"cuda:{dev}")
+            d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
+            d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+            d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+            g = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], mac="theta", theta=cfg["theta"],
+                       softening=cfg["softening"], precision=args.precision, device=dev,
+                       stream=side.cuda_stream, use_graphs=graphs)
+            g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+            g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+            g.leapfrog_device(d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
+                              d_pot.data_ptr(), 1e-3, refresh, "kdk", refresh)  # warm-up cycle
+            steps = refresh * 8
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(side)
+            g.leapfrog_device(d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
+                              d_pot.data_ptr(), 1e-3, steps, "kdk", refresh)
+            e1.record(side)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            res["graphs" if graphs else "launches"] = {"ms_per_step": ms, "bodies_per_s": n / (ms * 1e-3),
+                                                       "final_pos_checksum": float(d_pos.sum().item())}
+            g.close()
+    main = res["graphs"]
+    line = {"metric": METRIC, "value": main["bodies_per_s"], "unit": "bodies/s", "n_gpus": 1, "steps": refresh * 8,
+            "warmup": refresh, "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "dtype": "f64" if args.precision == "plain" else "f32+f64",
+            "config": {"workload": cfg["workload"] + f", KDK dt=1e-3, tree refreshed every {refresh} steps",
+                       "precision": args.precision},
+            "graphs": res, "speedup": res["launches"]["ms_per_step"] / main["ms_per_step"]}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ C3: same-error comparison
 # (p, theta, soft_gap): soft_gap > 0 keeps M2L pairs soft_gap * softening apart
 SWEEP_SETTINGS = ((12, 0.4, 0.0), (16, 0.4, 0.0), (12, 0.3, 0.0), (12, 0.4, 100.0), (12, 0.4, 300.0),
@@ -687,6 +742,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override N (small cases for profiling)")
+    ap.add_argument("--graphs", action="store_true",
+                    help="device leapfrog with tree reuse: launches against CUDA-graph replay")
     ap.add_argument("--sweep", action="store_true",
                     help="c3: force evaluations at several (p, theta) in both precisions, compared at p99 <= 1e-5")
     args = ap.parse_args()
@@ -711,6 +768,8 @@ def main():
     try:
         runner = {"c3": run_accuracy_sweep if args.sweep else run_kdk, "c4": run_ensemble,
                   "c5": run_serve}.get(args.config, run_gpu)
+        if args.graphs:
+            runner = run_graphs
         runner(args, cfg, rank, world, local_rank)
     finally:
         if world > 1:

@@ -96,6 +96,15 @@ struct fmmx_ctx {
     int nc = 0, nleaves = 0, nlevels = 0;
     int lvl_start[FMMX_NLEVELS + 1] = {0}, lvl_count[FMMX_NLEVELS + 1] = {0};
     bool built = false, evaluated = false, lists_valid = false;
+    // leapfrog steps on a reused tree, recorded once per tree as a CUDA graph
+    cudaGraphExec_t step_graph = nullptr;
+    const void* graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double graph_dt = 0.0;
+    int graph_scheme = -1;
+    void drop_graph() {
+        if (step_graph) cudaGraphExecDestroy(step_graph);
+        step_graph = nullptr;
+    }
     int n_m2l = 0, n_p2p = 0;
     unsigned long long pops = 0, p2p_inter = 0;
 
@@ -347,6 +356,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
     ctx->built = false;
     ctx->evaluated = false;
     ctx->lists_valid = false;
+    ctx->drop_graph();  // its kernels address the buffers and sizes of the old tree
     ctx->n = n;
     ctx->nsys = nsys;
     if (ctx->events) CK(cudaEventRecord(ctx->ev[0], s), "event");
@@ -677,14 +687,16 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
 // f pre-pass, walk or list build); moments and locals are recomputed from the
 // given positions about the cell centres of the last build. This is the
 // tree reuse of the reference's GPU backend (crates/visual/src/gpufmm.rs:9-20).
+// capture: the calls are being recorded into a CUDA graph (reuse only): no
+// timing events and no read-back at the end.
 fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot,
-                          bool reuse = false) {
+                          bool reuse = false, bool capture = false) {
     cudaStream_t s = ctx->stream;
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
     const int p = ctx->cfg.p, dim = dimp(p), nc = ctx->nc;
     const size_t n = ctx->n;
     cudaEvent_t* ev = ctx->ev;
-    const bool tm = ctx->events;
+    const bool tm = ctx->events && !capture;
     if (tm) CK(cudaEventRecord(ev[2], s), "event");
     ctx->launches = ctx->launches_build;
     if (d_pos == nullptr) d_pos = ctx->build_pos;
@@ -818,6 +830,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     CKL("l2p");
     }
     if (tm) CK(cudaEventRecord(ev[9], s), "event");
+    if (capture) return FMMX_OK;
     CK(cudaStreamSynchronize(s), "evaluate");
     CK(cudaMemcpy(&ctx->p2p_inter, ctx->inter.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "copy");
     if (tm) {
@@ -860,6 +873,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->p2p_tile = 0;
     c->preemptible = 0;
     c->soft_gap = 0.0;
+    c->use_graphs = 1;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -893,6 +907,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (c.p2p_tile < 0 || c.p2p_tile > 512) return FMMX_INVALID_ARG;
     if (c.preemptible != 0 && c.preemptible != 1) return FMMX_INVALID_ARG;
     if (!(c.soft_gap >= 0.0) || !std::isfinite(c.soft_gap)) return FMMX_INVALID_ARG;
+    if (c.use_graphs != 0 && c.use_graphs != 1) return FMMX_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -947,6 +962,7 @@ void fmmx_destroy(fmmx_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->cfg.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->drop_graph();
     for (int i = 0; i < 12; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1026,8 +1042,55 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, co
         d_pot = ctx->pot_out.p;
     }
     const unsigned g = grid_for(3 * n, 256);
+    const void* key[5] = {d_pos, d_vel, d_mass, d_acc, d_pot};
     for (int step = 0; step < nsteps; ++step) {
         const bool rebuild = (ctx->steps_since_build + 1) >= refresh_every;
+        // A step on a reused tree is the same sequence of launches every time:
+        // record it once as a CUDA graph and replay it (one launch instead of
+        // about 30). Not on the legacy default stream, which cannot be captured.
+        if (!rebuild && ctx->cfg.use_graphs && s != nullptr && ctx->lists_valid) {
+            const bool same = ctx->step_graph && ctx->graph_dt == dt && ctx->graph_scheme == scheme &&
+                              std::equal(key, key + 5, ctx->graph_key);
+            if (!same) {
+                ctx->drop_graph();
+                const bool ev_saved = ctx->events;
+                ctx->events = false;
+                cudaGraph_t graph = nullptr;
+                fmmx_status st = FMMX_OK;
+                if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                    st = cuda_fail(ctx, cudaGetLastError(), "graph capture");
+                if (st == FMMX_OK) {
+                    if (scheme == 0) {
+                        k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
+                        k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, dt);
+                    } else {
+                        k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, 0.5 * dt);
+                    }
+                    st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, true, true);
+                    if (scheme == 0) {
+                        k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
+                    } else {
+                        k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, dt);
+                        k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, 0.5 * dt);
+                    }
+                    const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+                    if (st == FMMX_OK && ec != cudaSuccess) st = cuda_fail(ctx, ec, "graph capture");
+                }
+                ctx->events = ev_saved;
+                if (st == FMMX_OK && cudaGraphInstantiate(&ctx->step_graph, graph, 0) != cudaSuccess) {
+                    ctx->step_graph = nullptr;
+                    st = cuda_fail(ctx, cudaGetLastError(), "graph instantiate");
+                }
+                if (graph) cudaGraphDestroy(graph);
+                if (st != FMMX_OK) return st;
+                std::copy(key, key + 5, ctx->graph_key);
+                ctx->graph_dt = dt;
+                ctx->graph_scheme = scheme;
+            }
+            if (cudaGraphLaunch(ctx->step_graph, s) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "graph");
+            ctx->steps_since_build++;
+            continue;
+        }
         if (scheme == 0) {  // kick-drift-kick; d_acc holds the forces at d_pos
             k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
             k_drift<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, dt);

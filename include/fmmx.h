@@ -79,6 +79,8 @@ typedef struct fmmx_config {
                           at least soft_gap * softening apart (r - rho_A - rho_B), on top of the MAC. The far
                           field uses the unsoftened kernel, which errs by about softening^2 / (2 d^2) relative
                           at distance d; this bounds that error. 0 (default): no such condition */
+    int use_graphs;    /* 1 (default): fmmx_leapfrog_device records a step on a reused tree (refresh_every > 1)
+                          as a CUDA graph once per tree and replays it; 0: plain launches */
 } fmmx_config;
 
 typedef struct fmmx_stats {

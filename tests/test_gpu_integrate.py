@@ -106,3 +106,24 @@ def test_kdk_matches_host_loop(precision, refresh):
     assert np.max(np.abs(x - hx)) < tol * scale
     rel = np.linalg.norm(a - ha, axis=1) / np.linalg.norm(ha, axis=1)
     assert np.percentile(rel, 99) < (1e-11 if refresh == 1 else 1e-4)
+
+
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_graph_replay_matches_launches(precision):
+    """Steps on a reused tree replayed from a CUDA graph give the bits of the
+    same steps launched one by one (refresh every 4 steps: captures after
+    every rebuild, replays in between)."""
+    import fmms_b200 as fx
+
+    import torch
+
+    mass, pos, vel = fx.gen_plummer_ic(8192, seed=9)
+    out = []
+    side = torch.cuda.Stream()  # the legacy default stream cannot be captured
+    for graphs in (False, True):
+        kw = dict(p=8, eps=0.0, n_leaf=32, mac="theta", theta=0.5, softening=1e-3, precision=precision,
+                  use_graphs=graphs)
+        with torch.cuda.stream(side):
+            out.append(run_leapfrog(mass, pos, vel, kw, 1e-3, 11, "kdk", 4))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
