@@ -128,9 +128,24 @@ __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, cons
     typedef cplx<T> Z;
     constexpr int N = K + 1;
     T vr[N], vi[N];
+    // FP32 half layout with an even entry count per cell: every cell starts on
+    // 16 bytes, so entry pairs that start on an even index load as one float4
+    Z Mv[N];
+    constexpr bool PAIRS = sizeof(T) == 4 && !FULL_LAYOUT && ((P + 1) * (P + 2) / 2) % 2 == 0;
+    constexpr int B0 = rot_hx(K, 0);
+    Unroll<0, T, N>::run([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        if constexpr (PAIRS && ((B0 + j) & 1) == 0 && j + 1 < N) {
+            const float4 v = *reinterpret_cast<const float4*>(ms + B0 + j);
+            Mv[j] = mk<T>(v.x, v.y);
+            Mv[j + 1] = mk<T>(v.z, v.w);
+        } else if constexpr (!PAIRS || ((B0 + j) & 1) == 0 || j == 0) {
+            Mv[j] = ms[FULL_LAYOUT ? (K * (K + 1) + j) : rot_hx(K, j)];
+        }
+    });
     Unroll<0, T, N>::run([&](auto mc) {
         constexpr int m = decltype(mc)::value;
-        const Z M = ms[FULL_LAYOUT ? (K * (K + 1) + m) : rot_hx(K, m)];
+        const Z M = Mv[m];
         const Z ph = ph_.A(m);
         T ur = ph.re * M.re + ph.im * M.im;  // ph * conj(M)
         T ui = ph.im * M.re - ph.re * M.im;
