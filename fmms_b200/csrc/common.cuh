@@ -62,6 +62,13 @@ __host__ __device__ __forceinline__ cplx<T> zconj(cplx<T> a) {
 // The tables cover every order up to FMMX_MAXP, so they are the same for all
 // contexts: a context created with another p re-uploads identical contents
 // and never changes the tables under a live context.
+// Cell stride of the mixed form's half-layout expansions: (p+1)(p+2)/2 entries
+// rounded up to even, so every cell starts on 16 bytes (FP32 complex) and the
+// M2L can load entry pairs as float4. The padding entry is never read.
+__host__ __device__ constexpr int half_stride(int p) {
+    return (p + 1) * (p + 2) / 2 + (((p + 1) * (p + 2) / 2) & 1);
+}
+
 struct OrderTables {
     double fact[2 * FMMX_MAXP + 1];             // j!, j = 0..2 FMMX_MAXP (moments.rs:11-17)
     double binom[FMMX_MAXP + 1][FMMX_MAXP + 1]; // binom[p][k] = C(p, k) as p!/(k!(p-k)!) (moments.rs:20-27)

@@ -645,12 +645,12 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
 fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirList& lp, double* d_acc,
                                     double* d_pot) {
     cudaStream_t s = ctx->stream;
-    const int p = ctx->cfg.p, nc = ctx->nc, H = (p + 1) * (p + 2) / 2;
+    const int p = ctx->cfg.p, nc = ctx->nc;
     const size_t n = ctx->n;
     const CellsView cv = view(ctx);
     cudaEvent_t* ev = ctx->ev;
     const bool tm = ctx->events;
-    CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * H * sizeof(zf), s), "memset");
+    CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * half_stride(p) * sizeof(zf), s), "memset");
     if (ctx->n_m2l > 0) {
         if (p > kRotwMaxP) return fail(ctx, FMMX_INVALID_ARG, "mixed precision supports p <= 16");
         int* work = nullptr;  // preemptible: one block per destination cell
@@ -715,8 +715,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     const int H = (p + 1) * (p + 2) / 2;
     const CellsView cv = view(ctx);
     if (mixed) {
-        CK(ctx->mom_f.ensure((size_t)nc * H), "alloc expansions");
-        CK(ctx->loc_f.ensure((size_t)nc * H), "alloc expansions");
+        CK(ctx->mom_f.ensure((size_t)nc * half_stride(p)), "alloc expansions");
+        CK(ctx->loc_f.ensure((size_t)nc * half_stride(p)), "alloc expansions");
         CK(ctx->ell.ensure(nc), "alloc expansions");
         CK(ctx->ellf.ensure(nc), "alloc expansions");
         k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_h.p, ctx->ell.p, ctx->ellf.p);

@@ -128,10 +128,11 @@ __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, cons
     typedef cplx<T> Z;
     constexpr int N = K + 1;
     T vr[N], vi[N];
-    // FP32 half layout with an even entry count per cell: every cell starts on
-    // 16 bytes, so entry pairs that start on an even index load as one float4
+    // FP32 half layout: every cell starts on 16 bytes (the cell stride is
+    // half_stride(P), even), so entry pairs that start on an even index load
+    // as one float4
     Z Mv[N];
-    constexpr bool PAIRS = sizeof(T) == 4 && !FULL_LAYOUT && ((P + 1) * (P + 2) / 2) % 2 == 0;
+    constexpr bool PAIRS = sizeof(T) == 4 && !FULL_LAYOUT;
     constexpr int B0 = rot_hx(K, 0);
     Unroll<0, T, N>::run([&](auto jc) {
         constexpr int j = decltype(jc)::value;
@@ -354,7 +355,7 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
                 sa = (T)iR;
                 sb = (T)iR;
             }
-            const Z* ms = mom + (size_t)src * (FULL_LAYOUT ? DIM : H);
+            const Z* ms = mom + (size_t)src * (FULL_LAYOUT ? DIM : half_stride(P));
             const T cap = SCALED ? T(1e30) : T(INFINITY);
             if constexpr (PH_REGS) {
                 rotw_back<T, P, FULL_LAYOUT>(ms, phr, col, sa, cap);
@@ -400,7 +401,7 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
                     out[n * (n + 1) - m] = mk<T>(sg * acc_re[t], -sg * acc_im[t]);
                 }
             } else {
-                loc[(size_t)c * H + e] = mk<T>(acc_re[t], acc_im[t]);
+                loc[(size_t)c * half_stride(P) + e] = mk<T>(acc_re[t], acc_im[t]);
             }
         }
     }

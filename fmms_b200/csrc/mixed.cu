@@ -76,7 +76,7 @@ __global__ void k_cell_scale(int nc, const double* __restrict__ rho, const doubl
 // FP64 full-layout moments (the exact upward pass) -> normalised FP32 half layout.
 __global__ void k_moments_to_mixed(int nc, int p, const zd* __restrict__ full, const double* __restrict__ ell,
                                    zf* __restrict__ half) {
-    const int H = (p + 1) * (p + 2) / 2, D = (p + 1) * (p + 1);
+    const int H = (p + 1) * (p + 2) / 2, D = (p + 1) * (p + 1), HS = half_stride(p);
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)nc * H;
          i += (size_t)gridDim.x * blockDim.x) {
         const int c = (int)(i / H), e = (int)(i % H);
@@ -84,7 +84,7 @@ __global__ void k_moments_to_mixed(int nc, int p, const zd* __restrict__ full, c
         split_h(e, n, m);
         const double s = pow(ell[c], -n);
         const zd v = full[(size_t)c * D + n * (n + 1) + m];
-        half[i] = mk<float>((float)(v.re * s), (float)(v.im * s));
+        half[(size_t)c * HS + e] = mk<float>((float)(v.re * s), (float)(v.im * s));
     }
 }
 
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
                     split_h(e, n, mm);
                     const cplx<A>* uo = u + o * H;
                     const A ratio = (A)(ell[ch] * il);
-                    const zf* mcv = mom + (size_t)ch * H;
+                    const zf* mcv = mom + (size_t)ch * half_stride(p);
                     A rpow = 1;  // ratio^{n-k}, built from k = n down
                     for (int k = n; k >= 0; --k) {
                         const int nk = n - k;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
             }
         }
         __syncthreads();
-        zf* out = mom + (size_t)c * H;
+        zf* out = mom + (size_t)c * half_stride(p);
         for (int e = tid; e < H; e += UPM_BLOCK) {
             A sr = 0, si = 0;
             for (int q = 0; q < nparts; ++q) {
@@ -230,11 +230,11 @@ __global__ void __launch_bounds__(128) k_l2l_mixed(const int32_t* __restrict__ l
         const A rx = (A)((cv.cx[par] - cv.cx[c]) * il), ry = (A)((cv.cy[par] - cv.cy[c]) * il),
                 rz = (A)((cv.cz[par] - cv.cz[c]) * il);
         if (tid <= p) ups_column<A>(rx, ry, rz, rx * rx + ry * ry + rz * rz, p, tid, u);
-        const zf* lp = loc + (size_t)par * H;
+        const zf* lp = loc + (size_t)par * half_stride(p);
         for (int e = tid; e < H; e += blockDim.x) fp[e] = lp[e];
         __syncthreads();
         const A ratio = (A)(ell[c] * il);
-        zf* lc = loc + (size_t)c * H;
+        zf* lc = loc + (size_t)c * half_stride(p);
         for (int e = tid; e < H; e += blockDim.x) {
             int n, m;
             split_h(e, n, m);
@@ -274,14 +274,13 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
                             const double* __restrict__ z, const double* __restrict__ nax,
                             const double* __restrict__ nay, const double* __restrict__ naz,
                             const double* __restrict__ npot, double* __restrict__ acc, double* __restrict__ pot) {
-    const int H = (p + 1) * (p + 2) / 2;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
         const int c = body_leaf[k];
         const double l = ell[c], il = 1.0 / l;
         const float rx = (float)((cv.cx[c] - x[k]) * il), ry = (float)((cv.cy[c] - y[k]) * il),
                     rz = (float)((cv.cz[c] - z[k]) * il);
         const float r2 = rx * rx + ry * ry + rz * rz;
-        const zf* L = loc + (size_t)c * H;
+        const zf* L = loc + (size_t)c * half_stride(p);
         float p00 = 0, p11r = 0, p11i = 0, p10 = 0;
         zf d = mk<float>(1.f, 0.f);
         for (int lm = 0; lm <= p; ++lm) {
