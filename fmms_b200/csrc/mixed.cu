@@ -348,13 +348,23 @@ __device__ __forceinline__ void ds_add(DS& a, float b) {
     a.lo += err;
 }
 
+// The hardware reciprocal square root (about 2^-22 relative error), flushing
+// subnormal inputs: r2 is a squared distance plus the squared softening, far
+// above the subnormal range whenever it is positive. The Newton step that
+// follows brings it to FP32 accuracy.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // One source body against one target, FP32, d relative to the target leaf's
 // centre; rsqrt plus one Newton step.
 __device__ __forceinline__ void p2p_term(const float4 s, float xi, float yi, float zi, float soft2, float& ax,
                                          float& ay, float& az, float& pt) {
     const float dx = s.x - xi, dy = s.y - yi, dz = s.z - zi;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
-    float inv = rsqrtf(r2);
+    float inv = rsqrt_approx(r2);
     inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
     const float mi = s.w * inv;
     const float f = mi * inv * inv;
