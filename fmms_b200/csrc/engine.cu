@@ -152,6 +152,8 @@ struct fmmx_ctx {
 
     // directed lists
     DBuf<uint64_t> m2l_keys, m2l_keys_s, p2p_keys, p2p_keys_s;
+    DBuf<uint32_t> m2l_k32, m2l_k32_s, p2p_k32, p2p_k32_s;  // the same when 2 * list_shift <= 32
+    bool keys32 = false;
     int list_shift = 32;  // keys of the directed lists: (dst << list_shift) | src
     DBuf<uint32_t> m2l_seg_b, m2l_seg_e, p2p_seg_b, p2p_seg_e;
 
@@ -595,7 +597,9 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     const int nc = ctx->nc;
     const int shift = bits_for((uint64_t)nc);  // keys (dst << shift) | src
     const int cbits = 2 * shift;
+    const bool k32 = cbits <= 32;  // 32-bit keys: half the sort traffic
     ctx->list_shift = shift;
+    ctx->keys32 = k32;
     // M2L
     const int nm = ctx->n_m2l;
     CK(ctx->m2l_seg_b.ensure(nc), "alloc lists");
@@ -603,15 +607,25 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->m2l_seg_b.p, 0, nc * sizeof(uint32_t), s), "memset");
     CK(cudaMemsetAsync(ctx->m2l_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
     if (nm > 0) {
-        CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
-        CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
-        k_expand_m2l<<<grid_for(nm, 256), 256, 0, s>>>(ctx->m2l.p, nm, shift, ctx->m2l_keys.p);
         LCOUNT(3);
-        size_t tb = sort_keys_u64_temp(2 * nm, cbits);
-        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-        CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
-        k_segments<<<grid_for(2 * (size_t)nm, 256), 256, 0, s>>>(ctx->m2l_keys_s.p, 2 * nm, shift, ctx->m2l_seg_b.p,
-                                                                 ctx->m2l_seg_e.p);
+        const unsigned ge = grid_for(nm, 256), gs = grid_for(2 * (size_t)nm, 256);
+        if (k32) {
+            CK(ctx->m2l_k32.ensure(2 * (size_t)nm), "alloc lists");
+            CK(ctx->m2l_k32_s.ensure(2 * (size_t)nm), "alloc lists");
+            launch_expand_m2l<uint32_t>(ge, s, ctx->m2l.p, nm, shift, ctx->m2l_k32.p);
+            size_t tb = sort_keys_u32_temp(2 * nm, cbits);
+            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+            CK(sort_keys_u32(ctx->cub_tmp.p, tb, ctx->m2l_k32.p, ctx->m2l_k32_s.p, 2 * nm, cbits, s), "m2l sort");
+            launch_segments<uint32_t>(gs, s, ctx->m2l_k32_s.p, 2 * nm, shift, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p);
+        } else {
+            CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
+            CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
+            launch_expand_m2l<uint64_t>(ge, s, ctx->m2l.p, nm, shift, ctx->m2l_keys.p);
+            size_t tb = sort_keys_u64_temp(2 * nm, cbits);
+            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+            CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
+            launch_segments<uint64_t>(gs, s, ctx->m2l_keys_s.p, 2 * nm, shift, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p);
+        }
         CKL("m2l lists");
     }
     // P2P
@@ -623,18 +637,29 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->p2p_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
     CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
     if (np > 0) {
-        CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
-        CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
         const uint64_t sentinel = (uint64_t)nc << shift;  // above every valid key, within 2 * shift bits
         LCOUNT(3);
-        k_expand_p2p<<<grid_for(np, 256), 256, 0, s>>>(ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
-                                                       ctx->inter.p);
-        size_t tb = sort_keys_u64_temp(2 * np, cbits);
-        CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-        CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->p2p_keys.p, ctx->p2p_keys_s.p, 2 * np, cbits, s), "p2p sort");
         const int nvalid = 2 * np - ctx->nleaves;
-        k_segments<<<grid_for(nvalid, 256), 256, 0, s>>>(ctx->p2p_keys_s.p, nvalid, shift, ctx->p2p_seg_b.p,
-                                                         ctx->p2p_seg_e.p);
+        const unsigned ge = grid_for(np, 256), gs = grid_for(nvalid, 256);
+        if (k32) {
+            CK(ctx->p2p_k32.ensure(2 * (size_t)np), "alloc lists");
+            CK(ctx->p2p_k32_s.ensure(2 * (size_t)np), "alloc lists");
+            launch_expand_p2p<uint32_t>(ge, s, ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_k32.p,
+                                        ctx->inter.p);
+            size_t tb = sort_keys_u32_temp(2 * np, cbits);
+            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+            CK(sort_keys_u32(ctx->cub_tmp.p, tb, ctx->p2p_k32.p, ctx->p2p_k32_s.p, 2 * np, cbits, s), "p2p sort");
+            launch_segments<uint32_t>(gs, s, ctx->p2p_k32_s.p, nvalid, shift, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p);
+        } else {
+            CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
+            CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
+            launch_expand_p2p<uint64_t>(ge, s, ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
+                                        ctx->inter.p);
+            size_t tb = sort_keys_u64_temp(2 * np, cbits);
+            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+            CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->p2p_keys.p, ctx->p2p_keys_s.p, 2 * np, cbits, s), "p2p sort");
+            launch_segments<uint64_t>(gs, s, ctx->p2p_keys_s.p, nvalid, shift, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p);
+        }
         CKL("p2p lists");
     }
     return FMMX_OK;
@@ -775,8 +800,11 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     }
     if (tm) CK(cudaEventRecord(ev[5], s), "event");
 
-    DirList lm{ctx->m2l_keys_s.p, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p, ctx->list_shift};
-    DirList lp{ctx->p2p_keys_s.p, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p, ctx->list_shift};
+    const bool k32 = ctx->keys32;
+    DirList lm{k32 ? nullptr : ctx->m2l_keys_s.p, k32 ? ctx->m2l_k32_s.p : nullptr, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p,
+               ctx->list_shift};
+    DirList lp{k32 ? nullptr : ctx->p2p_keys_s.p, k32 ? ctx->p2p_k32_s.p : nullptr, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p,
+               ctx->list_shift};
     if (mixed) {
         fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot);
         if (ms != FMMX_OK) return ms;

@@ -55,10 +55,12 @@ struct WalkBufs {
 // Segmented directed interaction list: for destination cell c, sources
 // src[seg_begin[c] .. seg_end[c]) (ascending).
 struct DirList {
-    const uint64_t* keys;  // (dst << shift) | src, sorted; shift = bits of the cell count
+    const uint64_t* keys;    // (dst << shift) | src, sorted; shift = bits of the cell count
+    const uint32_t* keys32;  // the same in 32 bits when 2 * shift <= 32 (then keys is null)
     const uint32_t* seg_begin;
     const uint32_t* seg_end;
     int shift;
+    __host__ __device__ uint64_t key(size_t i) const { return keys32 ? (uint64_t)keys32[i] : keys[i]; }
     __host__ __device__ uint32_t src(uint64_t key) const { return (uint32_t)(key & ((1ull << shift) - 1)); }
 };
 
@@ -94,10 +96,16 @@ __global__ void k_fprepass(CellsView cells, const double* x, const double* y, co
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
 
 // lists.cu
-__global__ void k_expand_m2l(const uint2* pairs, int np, int shift, uint64_t* keys);
-__global__ void k_expand_p2p(const uint2* pairs, int np, int shift, const uint32_t* count, uint64_t sentinel, uint64_t* keys,
-                             unsigned long long* interactions);
-__global__ void k_segments(const uint64_t* keys, int nkeys, int shift, uint32_t* seg_begin, uint32_t* seg_end);
+// Directed list keys from the walk's mutual pairs, with K = uint32_t or
+// uint64_t keys (launchers in lists.cu).
+template <typename K>
+void launch_expand_m2l(unsigned grid, cudaStream_t s, const uint2* pairs, int np, int shift, K* keys);
+template <typename K>
+void launch_expand_p2p(unsigned grid, cudaStream_t s, const uint2* pairs, int np, int shift, const uint32_t* count,
+                       uint64_t sentinel, K* keys, unsigned long long* interactions);
+template <typename K>
+void launch_segments(unsigned grid, cudaStream_t s, const K* keys, int nkeys, int shift, uint32_t* seg_begin,
+                     uint32_t* seg_end);
 
 // m2l.cu
 void upload_tables_m2l(const OrderTables& t, cudaStream_t s);

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(M2L_BLOCK) k_m2l_naive_f64(DirList L, int ncel
 #pragma unroll
         for (int j = 0; j < M2L_OUT; ++j) fr[j] = fi[j] = 0.0;
         for (uint32_t s = beg; s < end; ++s) {
-            const int src = (int)L.src(L.keys[s]);
+            const int src = (int)L.src(L.key(s));
             const double rx = bx - cv.cx[src], ry = by - cv.cy[src], rz = bz - cv.cz[src];
             if (tid <= p) {
                 const double r2 = rx * rx + ry * ry + rz * rz;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(M2L_BLOCK) k_m2l_rot_f64(DirList L, int ncells
 #pragma unroll
         for (int j = 0; j < M2L_OUT; ++j) fr[j] = fi[j] = 0.0;
         for (uint32_t s = beg; s < end; ++s) {
-            const int src = (int)L.src(L.keys[s]);
+            const int src = (int)L.src(L.key(s));
             const double rx = bx - cv.cx[src], ry = by - cv.cy[src], rz = bz - cv.cz[src];
             const double r2 = rx * rx + ry * ry + rz * rz;
             const double alpha = atan2(ry, rx);

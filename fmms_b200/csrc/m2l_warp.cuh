@@ -296,8 +296,7 @@ __device__ __noinline__ void rotw_fwd_ni(cplx<T>* col, const cplx<T>* pa, const 
 }
 
 template <typename T, int P, bool SCALED, bool FULL_LAYOUT>
-__device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, const uint64_t* __restrict__ keys,
-                                          uint64_t smask,
+__device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, const DirList& L,
                                           const CellsView& cv, const T* __restrict__ scale,
                                           const cplx<T>* __restrict__ mom, cplx<T>* __restrict__ loc,
                                           cplx<T>* __restrict__ sbuf, int lane) {
@@ -316,7 +315,7 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
     for (uint32_t chunk = beg; chunk < end; chunk += 32) {
         const int nact = (int)min(32u, end - chunk);
         if (lane < nact) {
-            const int src = (int)(keys[chunk + lane] & smask);
+            const int src = (int)L.src(L.key(chunk + lane));
             // geometry in FP64: r = s_B - z_A
             const double rx = bx - cv.cx[src], ry = by - cv.cy[src], rz = bz - cv.cz[src];
             const double rxy2 = rx * rx + ry * ry;
@@ -428,7 +427,7 @@ __global__ void __launch_bounds__(32) k_m2l_rotw(DirList L, int ncells, CellsVie
         const int c = blockIdx.x;
         if (c >= ncells) return;
         const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
-        if (beg < end) rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L.keys, (1ull << L.shift) - 1, cv, scale, mom, loc, sbuf, lane);
+        if (beg < end) rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L, cv, scale, mom, loc, sbuf, lane);
         return;
     }
     for (;;) {
@@ -438,7 +437,7 @@ __global__ void __launch_bounds__(32) k_m2l_rotw(DirList L, int ncells, CellsVie
         if (c >= ncells) break;
         const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
         if (beg >= end) continue;
-        rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L.keys, (1ull << L.shift) - 1, cv, scale, mom, loc, sbuf, lane);
+        rotw_body<T, P, SCALED, FULL_LAYOUT>(c, beg, end, L, cv, scale, mom, loc, sbuf, lane);
     }
 }
 

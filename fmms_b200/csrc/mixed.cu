@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                     const int q = q0 + tid;
                     uint32_t v = 0;
                     if (q < ns) {
-                        const int src = (int)L.src(L.keys[sc + q]);
+                        const int src = (int)L.src(L.key(sc + q));
                         v = cv.count[src];
                         sfirst[q] = cv.first[src];
                     }
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                     for (int w = 0; w < wid; ++w) base += wsum[w];
                     if (q < ns) {
                         pre[q + 1] = base + incl;
-                        if ((int)L.src(L.keys[sc + q]) == c) self_pos = (int)(base + incl - v);
+                        if ((int)L.src(L.key(sc + q)) == c) self_pos = (int)(base + incl - v);
                     }
                     if (q0 == 0 && tid == 0) pre[0] = 0;
                     __syncthreads();

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(P2P_BLOCK) k_p2p_f64(DirList L, int ncells, Ce
                 __syncthreads();
                 // exclusive prefix of the chunk's source leaf sizes
                 for (int q = tid; q < ns; q += P2P_BLOCK) {
-                    const int src = (int)L.src(L.keys[sc + q]);
+                    const int src = (int)L.src(L.key(sc + q));
                     pre[q + 1] = cv.count[src];
                     sfirst[q] = cv.first[src];
                 }

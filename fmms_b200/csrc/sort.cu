@@ -33,6 +33,17 @@ cudaError_t sort_keys_u64(void* tmp, size_t tmp_bytes, const uint64_t* kin, uint
     return cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, n, 0, end_bit, s);
 }
 
+size_t sort_keys_u32_temp(int n, int end_bit) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, n, 0, end_bit);
+    return bytes;
+}
+
+cudaError_t sort_keys_u32(void* tmp, size_t tmp_bytes, const uint32_t* kin, uint32_t* kout, int n, int end_bit,
+                          cudaStream_t s) {
+    return cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, n, 0, end_bit, s);
+}
+
 // Independent sorts of the segments [off[s], off[s+1]) (a forest of systems).
 size_t sort_pairs_seg_temp(int n, int nseg, const uint64_t* off, int end_bit) {
     size_t bytes = 0;
