@@ -293,7 +293,7 @@ class _NullCtx:
 # directed translations); the expansions are L2-resident, so the traffic grows
 # with the translation count. See profiles/m2l_rotw_f32_p10_n262144.md and
 # profiles/m2l_rotw_f64_p10_n262144.md.
-M2L_DRAM_BYTES_PER_TRANSLATION = {("mixed", 10): (57.778432e6 + 1.495296e6) / 5809554,
+M2L_DRAM_BYTES_PER_TRANSLATION = {("mixed", 10): (34.537728e6 + 0.07424e6) / 5809554,
                                   ("plain", 10): (84.023808e6 + 21.590272e6) / 5809554}
 
 
