@@ -30,7 +30,8 @@ calibrated extra latency (the larger of the two system types) -- stays within
 `headroom` times the isolated latency (the smaller of the two types) of the
 batch's smallest session, and only while the lane's recent steps stay within
 that bound (feedback against prediction error). The joining tick measures the
-prediction: if it took longer than `headroom` times the isolated latency of the
+prediction: its ratio to the prediction (kept >= 1, decaying) scales later
+predictions, and if it took longer than `headroom` times the isolated latency of the
 batch's smallest session, the sessions that joined in it (all of them when
 others were already stepping, else all but the first) -- which have not
 stepped yet, so nothing of theirs changes -- go back to the front of the queue
@@ -159,6 +160,7 @@ class Lane:
         self.tick_ms: list[float] = []  # device time of each tick
         self.last_interval_ms = None  # wall interval of the last tick that stepped sessions
         self.predicted_ms = None  # predicted interval after the last admission, until measured
+        self.corr = 1.0  # >= 1: measured over predicted latency of recent joining ticks
         self.recent_ratio: deque[float] = deque(maxlen=8)
         self.bodies_stepped = 0
         self.departures = 0  # sessions finished in this lane
@@ -195,7 +197,7 @@ class Lane:
             fits = s.retry_after < self.departures
             if fits and model is not None and nmin is not None:
                 pred = (tau if tau is not None else model.iso(nmin)) + model.extra(s.n)
-                fits = pred <= srv.headroom * model.iso(min(nmin, s.n))
+                fits = pred * self.corr <= srv.headroom * model.iso(min(nmin, s.n))
             if fits and srv.reserve(s.bytes_needed()):
                 self.queue.remove(s)
                 s.admitted_at = now
@@ -328,6 +330,7 @@ class Lane:
                 s.step_ms.append(1e3 * (t_end - s.last_end))
                 s.last_end = t_end
                 self.bodies_stepped += s.n
+            predicted = self.predicted_ms
             if stepping:
                 self.last_interval_ms = max(s.step_ms[-1] for s in stepping)
                 self.predicted_ms = None
@@ -336,6 +339,10 @@ class Lane:
             joined = [s for s in self.members if not s.primed]
             model = self.srv.model
             if joined and model is not None and len(self.members) > 1:
+                # learn how far the model under-predicts joins (decaying toward 1)
+                if predicted:
+                    seen = 1e3 * (t_end - t_start) / predicted
+                    self.corr = min(4.0, max(1.0, 0.9 * self.corr, seen))
                 ratio = 1e3 * (t_end - t_start) / model.iso(min(s.n for s in self.members))
                 undo = joined if stepping else joined[1:]
                 if ratio > self.srv.headroom and undo:
