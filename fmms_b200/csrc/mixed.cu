@@ -111,6 +111,8 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
     const int P1 = p + 1;
     cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw);  // 8 x H: Υ of the child offsets
     cplx<A>* part = u + 8 * H;                          // 8 x H: partial sums
+    zf* cm = reinterpret_cast<zf*>(part + 8 * H);       // 8 x H: the children's moments
+    A* bod = reinterpret_cast<A*>(cm + 8 * H);          // 4 x UPM_BLOCK: a chunk of the leaf's bodies
     const int tid = threadIdx.x;
     const int G = min(8, UPM_BLOCK / P1);
     for (int j = blockIdx.x; j < lcnt; j += gridDim.x) {
@@ -121,14 +123,26 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
         if (cv.leaf[c]) {
             nparts = G;
             const int mc = tid % P1, g = tid / P1;
-            if (g < G) {
-                cplx<A>* acc = part + g * H;  // this thread's entries hx(n, mc), n >= mc
+            cplx<A>* acc = part + g * H;  // this thread's entries hx(n, mc), n >= mc
+            if (g < G)
                 for (int n = mc; n <= p; ++n) acc[hx(n, mc)] = mk<A>(A(0), A(0));
-                const uint32_t f = cv.first[c], cnt = cv.count[c];
-                for (uint32_t b = g; b < cnt; b += G) {
-                    const A rx = (A)((x[f + b] - sx) * il), ry = (A)((y[f + b] - sy) * il),
-                            rz = (A)((z[f + b] - sz) * il);
-                    const A mb = (A)m[f + b];
+            const uint32_t f = cv.first[c], cnt = cv.count[c];
+            for (uint32_t b0 = 0; b0 < cnt; b0 += UPM_BLOCK) {
+                // the chunk's bodies, relative and scaled, loaded by all threads at once
+                const uint32_t nb = min((uint32_t)UPM_BLOCK, cnt - b0);
+                __syncthreads();
+                if ((uint32_t)tid < nb) {
+                    const uint32_t q = f + b0 + tid;
+                    bod[tid] = (A)((x[q] - sx) * il);
+                    bod[UPM_BLOCK + tid] = (A)((y[q] - sy) * il);
+                    bod[2 * UPM_BLOCK + tid] = (A)((z[q] - sz) * il);
+                    bod[3 * UPM_BLOCK + tid] = (A)m[q];
+                }
+                __syncthreads();
+                if (g >= G) continue;
+                for (uint32_t b = g; b < nb; b += G) {
+                    const A rx = bod[b], ry = bod[UPM_BLOCK + b], rz = bod[2 * UPM_BLOCK + b];
+                    const A mb = bod[3 * UPM_BLOCK + b];
                     const A r2 = rx * rx + ry * ry + rz * rz;
                     cplx<A> d = mk<A>(A(1), A(0));
                     for (int q = 1; q <= mc; ++q) d = zmul(zscale(mk<A>(rx, ry), (A)c_tab.inv2m[q]), d);
@@ -155,6 +169,11 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
                         dz = (A)((cv.cz[ch] - sz) * il);
                 ups_column<A>(dx, dy, dz, dx * dx + dy * dy + dz * dz, p, mc, u + o * H);
             }
+            for (int w = tid; w < 8 * H; w += UPM_BLOCK) {  // stage the children's moments
+                const int o = w / H, e = w % H;
+                const int ch = cv.child[8 * c + o];
+                if (ch >= 0) cm[w] = mom[(size_t)ch * half_stride(p) + e];
+            }
             __syncthreads();
             for (int w = tid; w < 8 * H; w += UPM_BLOCK) {
                 const int o = w / H, e = w % H;
@@ -165,7 +184,7 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
                     split_h(e, n, mm);
                     const cplx<A>* uo = u + o * H;
                     const A ratio = (A)(ell[ch] * il);
-                    const zf* mcv = mom + (size_t)ch * half_stride(p);
+                    const zf* mcv = cm + o * H;
                     A rpow = 1;  // ratio^{n-k}, built from k = n down
                     for (int k = n; k >= 0; --k) {
                         const int nk = n - k;
@@ -199,17 +218,22 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
     }
 }
 
+template <typename A>
+static size_t upward_smem(int H) {
+    return (size_t)16 * H * sizeof(cplx<A>) + (size_t)8 * H * sizeof(zf) + (size_t)4 * UPM_BLOCK * sizeof(A);
+}
+
 void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
                          int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,
                          const double* z, const double* m, int p, zf* mom) {
     (void)warps;
     const int H = (p + 1) * (p + 2) / 2;
     if (fp64)
-        k_upward_mixed<double><<<grid, UPM_BLOCK, (size_t)16 * H * sizeof(zd), s>>>(level_cells, lstart, lcnt, cv,
-                                                                                    ell, x, y, z, m, p, mom);
+        k_upward_mixed<double><<<grid, UPM_BLOCK, upward_smem<double>(H), s>>>(level_cells, lstart, lcnt, cv, ell, x,
+                                                                               y, z, m, p, mom);
     else
-        k_upward_mixed<float><<<grid, UPM_BLOCK, (size_t)16 * H * sizeof(zf), s>>>(level_cells, lstart, lcnt, cv,
-                                                                                   ell, x, y, z, m, p, mom);
+        k_upward_mixed<float><<<grid, UPM_BLOCK, upward_smem<float>(H), s>>>(level_cells, lstart, lcnt, cv, ell, x, y,
+                                                                             z, m, p, mom);
 }
 
 // L2L for the cells of one level (L >= 1), one CTA per cell; A as above.
