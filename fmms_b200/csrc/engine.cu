@@ -162,7 +162,11 @@ struct fmmx_ctx {
     uint64_t launches = 0, launches_build = 0;
 
     fmmx_stats st;
-    cudaEvent_t ev[12];
+    cudaEvent_t ev[16];
+    // second stream: the walk and the lists run beside the upward pass, the
+    // P2P beside the M2L and L2L; fork/join events order the two
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t fork[3] = {nullptr, nullptr, nullptr};
     bool events = false;
 };
 
@@ -517,8 +521,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
 }
 
 // ---------------------------------------------------------------- evaluate
-fmmx_status walk_impl(fmmx_ctx* ctx) {
-    cudaStream_t s = ctx->stream;
+fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
     const int nc = ctx->nc;
     // capacities follow the current tree (a context may see trees of very
     // different sizes, e.g. the forests of a serving loop) and grow on overflow
@@ -592,8 +595,7 @@ fmmx_status walk_impl(fmmx_ctx* ctx) {
     }
 }
 
-fmmx_status lists_impl(fmmx_ctx* ctx) {
-    cudaStream_t s = ctx->stream;
+fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
     const int nc = ctx->nc;
     const int shift = bits_for((uint64_t)nc);  // keys (dst << shift) | src
     const int cbits = 2 * shift;
@@ -668,13 +670,20 @@ fmmx_status lists_impl(fmmx_ctx* ctx) {
 // Mixed form: FP32 M2L/L2L/L2P on normalised expansions, FP32 + double-single
 // P2P; events 5..9 as in the plain path.
 fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirList& lp, double* d_acc,
-                                    double* d_pot) {
-    cudaStream_t s = ctx->stream;
+                                    double* d_pot, bool tm) {
+    cudaStream_t s = ctx->stream, s2 = ctx->stream2;
     const int p = ctx->cfg.p, nc = ctx->nc;
     const size_t n = ctx->n;
     const CellsView cv = view(ctx);
     cudaEvent_t* ev = ctx->ev;
-    const bool tm = ctx->events;
+    // near field on the second stream, beside the far field
+    if (tm) CK(cudaEventRecord(ev[12], s2), "event");
+    const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)nc, s2, lp, nc, cv,
+                     ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
+    CKL("p2p (mixed)");
+    if (tm) CK(cudaEventRecord(ev[8], s2), "event");
+    CK(cudaEventRecord(ctx->fork[2], s2), "event");
     CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * half_stride(p) * sizeof(zf), s), "memset");
     if (ctx->n_m2l > 0) {
         if (p > kRotwMaxP) return fail(ctx, FMMX_INVALID_ARG, "mixed precision supports p <= 16");
@@ -696,11 +705,8 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     }
     CKL("l2l (mixed)");
     if (tm) CK(cudaEventRecord(ev[7], s), "event");
-    const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)nc, s, lp, nc, cv,
-                     ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
-    CKL("p2p (mixed)");
-    if (tm) CK(cudaEventRecord(ev[8], s), "event");
+    CK(cudaStreamWaitEvent(s, ctx->fork[2], 0), "join");  // L2P adds the near field
+    if (tm) CK(cudaEventRecord(ev[13], s), "event");
     k_l2p_mixed<<<grid_for(n, 128), 128, 0, s>>>(n, ctx->body_leaf.p, ctx->order.p, cv, ctx->ell.p, p,
                                                  ctx->loc_f.p, ctx->x.p, ctx->y.p, ctx->z.p, ctx->nax.p,
                                                  ctx->nay.p, ctx->naz.p, ctx->npot.p, d_acc, d_pot);
@@ -716,7 +722,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
 // timing events and no read-back at the end.
 fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot,
                           bool reuse = false, bool capture = false) {
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = ctx->stream, s2 = ctx->stream2;
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
     const int p = ctx->cfg.p, dim = dimp(p), nc = ctx->nc;
     const size_t n = ctx->n;
@@ -746,6 +752,13 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CK(ctx->ellf.ensure(nc), "alloc expansions");
         k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_h.p, ctx->ell.p, ctx->ellf.p);
         LCOUNT(1);
+    }
+    // the second stream starts once the bodies are gathered (and, for the
+    // Dehnen MAC, whose walk reads the multipole power and fmin, after the
+    // upward pass)
+    if (!dehnen) {
+        CK(cudaEventRecord(ctx->fork[0], s), "event");
+        CK(cudaStreamWaitEvent(s2, ctx->fork[0], 0), "fork");
     }
     if (dehnen) {
         CK(cudaMemsetAsync(ctx->flags.p + 3, 0, sizeof(int), s), "memset");
@@ -783,8 +796,13 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         }
     }
     if (tm) CK(cudaEventRecord(ev[3], s), "event");
+    if (dehnen) {
+        CK(cudaEventRecord(ctx->fork[0], s), "event");
+        CK(cudaStreamWaitEvent(s2, ctx->fork[0], 0), "fork");
+    }
+    if (tm) CK(cudaEventRecord(ev[10], s2), "event");
     if (!reuse) {
-        fmmx_status st = walk_impl(ctx);
+        fmmx_status st = walk_impl(ctx, s2);
         if (st != FMMX_OK) return st;
         if (dehnen) {
             int bad = 0;
@@ -792,13 +810,16 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
             if (bad) return fail(ctx, FMMX_DEVICE_ERROR, "f pre-pass stack overflow");
         }
     }
-    if (tm) CK(cudaEventRecord(ev[4], s), "event");
+    if (tm) CK(cudaEventRecord(ev[4], s2), "event");
     if (!reuse) {
-        fmmx_status st = lists_impl(ctx);
+        fmmx_status st = lists_impl(ctx, s2);
         if (st != FMMX_OK) return st;
         ctx->lists_valid = true;
     }
-    if (tm) CK(cudaEventRecord(ev[5], s), "event");
+    if (tm) CK(cudaEventRecord(ev[5], s2), "event");
+    CK(cudaEventRecord(ctx->fork[1], s2), "event");
+    CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L reads the lists
+    if (tm) CK(cudaEventRecord(ev[11], s), "event");
 
     const bool k32 = ctx->keys32;
     DirList lm{k32 ? nullptr : ctx->m2l_keys_s.p, k32 ? ctx->m2l_k32_s.p : nullptr, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p,
@@ -806,9 +827,18 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     DirList lp{k32 ? nullptr : ctx->p2p_keys_s.p, k32 ? ctx->p2p_k32_s.p : nullptr, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p,
                ctx->list_shift};
     if (mixed) {
-        fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot);
+        fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot, tm);
         if (ms != FMMX_OK) return ms;
     } else {
+    {  // near field on the second stream, beside the far field
+        if (tm) CK(cudaEventRecord(ev[12], s2), "event");
+        const double soft2 = ctx->cfg.softening * ctx->cfg.softening;
+        k_p2p_f64<<<(unsigned)nc, 128, 0, s2>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2,
+                                                ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
+        CKL("p2p");
+        if (tm) CK(cudaEventRecord(ev[8], s2), "event");
+        CK(cudaEventRecord(ctx->fork[2], s2), "event");
+    }
     CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
     if (ctx->n_m2l > 0) {
         const unsigned g = std::min<unsigned>(nc, 148u * 16u);
@@ -844,14 +874,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CKL("l2l");
     }
     if (tm) CK(cudaEventRecord(ev[7], s), "event");
-    {
-        const double soft2 = ctx->cfg.softening * ctx->cfg.softening;
-        k_p2p_f64<<<(unsigned)nc, 128, 0, s>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p,
-                                                                      ctx->m.p, soft2, ctx->nax.p, ctx->nay.p,
-                                                                      ctx->naz.p, ctx->npot.p);
-        CKL("p2p");
-    }
-    if (tm) CK(cudaEventRecord(ev[8], s), "event");
+    CK(cudaStreamWaitEvent(s, ctx->fork[2], 0), "join");  // L2P adds the near field
+    if (tm) CK(cudaEventRecord(ev[13], s), "event");
     k_l2p_f64<<<grid_for(n, 128), 128, 0, s>>>(n, ctx->body_leaf.p, ctx->order.p, cv, p, ctx->locals.p, ctx->x.p,
                                                ctx->y.p, ctx->z.p, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p,
                                                d_acc, d_pot);
@@ -867,13 +891,14 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
             cudaEventElapsedTime(&ms, ev[a], ev[b]);
             return (double)ms;
         };
+        // stages on the two streams overlap: each is timed on its own stream
         ctx->st.ms_upward = el(2, 3);
-        ctx->st.ms_walk = el(3, 4);
+        ctx->st.ms_walk = el(10, 4);
         ctx->st.ms_lists = el(4, 5);
-        ctx->st.ms_m2l = el(5, 6);
+        ctx->st.ms_m2l = el(11, 6);
         ctx->st.ms_l2l = el(6, 7);
-        ctx->st.ms_p2p = el(7, 8);
-        ctx->st.ms_l2p = el(8, 9);
+        ctx->st.ms_p2p = el(12, 8);
+        ctx->st.ms_l2p = el(13, 9);
         ctx->st.ms_evaluate = el(2, 9);
     }
     ctx->evaluated = true;
@@ -956,7 +981,22 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
         ctx->own_stream = true;
     }
     ctx->events = true;
-    for (int i = 0; i < 12; ++i) cudaEventCreate(&ctx->ev[i]);
+    for (int i = 0; i < 16; ++i) cudaEventCreate(&ctx->ev[i]);
+    {
+        int prio = 0;
+        cudaStreamGetPriority(ctx->stream, &prio);
+        if (cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio) != cudaSuccess) {
+            cudaGetLastError();
+            fmmx_destroy(ctx);
+            return FMMX_DEVICE_ERROR;
+        }
+        for (int i = 0; i < 3; ++i)
+            if (cudaEventCreateWithFlags(&ctx->fork[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                fmmx_destroy(ctx);
+                return FMMX_DEVICE_ERROR;
+            }
+    }
     cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
     make_tables(ctx->tab);
     {
@@ -990,9 +1030,13 @@ void fmmx_destroy(fmmx_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->cfg.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
     ctx->drop_graph();
-    for (int i = 0; i < 12; ++i)
+    for (int i = 0; i < 16; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (int i = 0; i < 3; ++i)
+        if (ctx->fork[i]) cudaEventDestroy(ctx->fork[i]);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
