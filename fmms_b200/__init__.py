@@ -69,6 +69,7 @@ class Config(C.Structure):
         ("preemptible", C.c_int),
         ("soft_gap", C.c_double),
         ("use_graphs", C.c_int),
+        ("overlap", C.c_int),
     ]
 
 
@@ -189,7 +190,8 @@ class Fmm:
     def __init__(self, mass, pos, p: int = 8, eps: float = 1e-5, n_leaf: int = 16, *, mac: str = "dehnen",
                  theta: float = 0.5, softening: float = 0.0, precision: str = "plain", center: str = "com",
                  m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0,
-                 preemptible: bool = False, soft_gap: float = 0.0, use_graphs: bool = True):
+                 preemptible: bool = False, soft_gap: float = 0.0, use_graphs: bool = True,
+                 overlap: bool = True):
         cfg = Config()
         lib().fmmx_config_default(C.byref(cfg))
         cfg.p = int(p)
@@ -207,6 +209,7 @@ class Fmm:
         cfg.preemptible = 1 if preemptible else 0
         cfg.soft_gap = float(soft_gap)
         cfg.use_graphs = 1 if use_graphs else 0
+        cfg.overlap = 1 if overlap else 0
         self.cfg = cfg
         self.p = cfg.p
         h = _vp()

@@ -671,7 +671,7 @@ fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
 // P2P; events 5..9 as in the plain path.
 fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirList& lp, double* d_acc,
                                     double* d_pot, bool tm) {
-    cudaStream_t s = ctx->stream, s2 = ctx->stream2;
+    cudaStream_t s = ctx->stream, s2 = ctx->cfg.overlap ? ctx->stream2 : ctx->stream;
     const int p = ctx->cfg.p, nc = ctx->nc;
     const size_t n = ctx->n;
     const CellsView cv = view(ctx);
@@ -684,6 +684,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s2), "event");
     CK(cudaEventRecord(ctx->fork[2], s2), "event");
+    if (tm) CK(cudaEventRecord(ev[11], s), "event");  // far field from here
     CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * half_stride(p) * sizeof(zf), s), "memset");
     if (ctx->n_m2l > 0) {
         if (p > kRotwMaxP) return fail(ctx, FMMX_INVALID_ARG, "mixed precision supports p <= 16");
@@ -722,7 +723,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
 // timing events and no read-back at the end.
 fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot,
                           bool reuse = false, bool capture = false) {
-    cudaStream_t s = ctx->stream, s2 = ctx->stream2;
+    cudaStream_t s = ctx->stream, s2 = ctx->cfg.overlap ? ctx->stream2 : ctx->stream;
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
     const int p = ctx->cfg.p, dim = dimp(p), nc = ctx->nc;
     const size_t n = ctx->n;
@@ -819,7 +820,6 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     if (tm) CK(cudaEventRecord(ev[5], s2), "event");
     CK(cudaEventRecord(ctx->fork[1], s2), "event");
     CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L reads the lists
-    if (tm) CK(cudaEventRecord(ev[11], s), "event");
 
     const bool k32 = ctx->keys32;
     DirList lm{k32 ? nullptr : ctx->m2l_keys_s.p, k32 ? ctx->m2l_k32_s.p : nullptr, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p,
@@ -839,6 +839,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         if (tm) CK(cudaEventRecord(ev[8], s2), "event");
         CK(cudaEventRecord(ctx->fork[2], s2), "event");
     }
+    if (tm) CK(cudaEventRecord(ev[11], s), "event");  // far field from here
     CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
     if (ctx->n_m2l > 0) {
         const unsigned g = std::min<unsigned>(nc, 148u * 16u);
@@ -927,6 +928,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->preemptible = 0;
     c->soft_gap = 0.0;
     c->use_graphs = 1;
+    c->overlap = 1;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -961,6 +963,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (c.preemptible != 0 && c.preemptible != 1) return FMMX_INVALID_ARG;
     if (!(c.soft_gap >= 0.0) || !std::isfinite(c.soft_gap)) return FMMX_INVALID_ARG;
     if (c.use_graphs != 0 && c.use_graphs != 1) return FMMX_INVALID_ARG;
+    if (c.overlap != 0 && c.overlap != 1) return FMMX_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

@@ -81,6 +81,9 @@ typedef struct fmmx_config {
                           at distance d; this bounds that error. 0 (default): no such condition */
     int use_graphs;    /* 1 (default): fmmx_leapfrog_device records a step on a reused tree (refresh_every > 1)
                           as a CUDA graph once per tree and replays it; 0: plain launches */
+    int overlap;       /* 1 (default): an evaluation runs on two streams (walk and lists beside the upward pass,
+                          P2P beside M2L and L2L; the per-stage times then overlap); 0: one stream, every
+                          stage alone on the device (for timing single kernels) */
 } fmmx_config;
 
 typedef struct fmmx_stats {
