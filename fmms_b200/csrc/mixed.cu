@@ -228,12 +228,18 @@ void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, co
                          const double* z, const double* m, int p, zf* mom) {
     (void)warps;
     const int H = (p + 1) * (p + 2) / 2;
-    if (fp64)
-        k_upward_mixed<double><<<grid, UPM_BLOCK, upward_smem<double>(H), s>>>(level_cells, lstart, lcnt, cv, ell, x,
-                                                                               y, z, m, p, mom);
-    else
-        k_upward_mixed<float><<<grid, UPM_BLOCK, upward_smem<float>(H), s>>>(level_cells, lstart, lcnt, cv, ell, x, y,
-                                                                             z, m, p, mom);
+    // above 48 KB (FP64 levels from p = 14) the kernel must opt in to more shared memory
+    if (fp64) {
+        const size_t sm = upward_smem<double>(H);
+        if (sm > 48 * 1024)
+            cudaFuncSetAttribute(k_upward_mixed<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_upward_mixed<double><<<grid, UPM_BLOCK, sm, s>>>(level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+    } else {
+        const size_t sm = upward_smem<float>(H);
+        if (sm > 48 * 1024)
+            cudaFuncSetAttribute(k_upward_mixed<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_upward_mixed<float><<<grid, UPM_BLOCK, sm, s>>>(level_cells, lstart, lcnt, cv, ell, x, y, z, m, p, mom);
+    }
 }
 
 // L2L for the cells of one level (L >= 1), one CTA per cell; A as above.

@@ -16,7 +16,7 @@ def targets(n, k=2048, seed=5):
     return np.sort(np.random.default_rng(seed).choice(n, size=min(k, n), replace=False)).astype(np.uint32)
 
 
-@pytest.mark.parametrize("p,theta", [(4, 0.5), (8, 0.5), (10, 0.5), (12, 0.4)])
+@pytest.mark.parametrize("p,theta", [(4, 0.5), (8, 0.5), (10, 0.5), (12, 0.4), (14, 0.5), (16, 0.5)])
 def test_mixed_accuracy_plummer(p, theta):
     import fmms_b200 as fx
 
