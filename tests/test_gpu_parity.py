@@ -206,3 +206,30 @@ def test_momentum_conserved_gpu(orc):
     fsum = (mass[:, None] * res.accel).sum(0)
     ftot = (mass * np.linalg.norm(res.accel, axis=1)).sum()
     assert np.linalg.norm(fsum) / ftot < 1e-13
+
+
+def test_full_size_c2_plain(orc):
+    """The headline configuration at full size, N = 2^20 (uniform cube, log-normal
+    masses, softening 1e-4, p = 10, theta 0.5, leaf 64): Morton keys, slot order
+    and both pair sets equal to the oracle's, accelerations and potentials within
+    1e-12 relative per body (the oracle runs threaded on the host)."""
+    import os
+
+    mass, pos = fx().gen_uniform_lognormal(1 << 20, 0.5, 22)
+    kw = dict(mac="theta", theta=0.5, softening=1e-4)
+    g = fx().Fmm(mass, pos, 10, 0.0, 64, **kw)
+    res = g.run()
+    o = orc.Fmm(mass, pos, 10, 0.0, 64, mac=orc.MAC_THETA, theta=0.5, softening=1e-4)
+    acc_o, pot_o = o.run(nthreads=os.cpu_count() or 1)
+    order_g, keys_g, _ = g.export_tree()
+    order_o, keys_o = o.order()
+    assert np.array_equal(keys_g, keys_o)
+    assert np.array_equal(order_g, order_o)
+    m2l_g, p2p_g = g.export_lists()
+    m2l_o, p2p_o = o.lists()
+    assert np.array_equal(pair_set(m2l_g), pair_set(m2l_o))
+    assert np.array_equal(pair_set(p2p_g), pair_set(p2p_o))
+    ra = rel_rows(res.accel, acc_o)
+    rp = rel_rows(res.pot, pot_o)
+    assert ra.max() < ACC_TOL, f"acc rel err {ra.max():.3e}"
+    assert rp.max() < ACC_TOL, f"pot rel err {rp.max():.3e}"
