@@ -82,3 +82,24 @@ def test_mixed_dehnen_lists_match_plain(orc):
         assert np.array_equal(sa, sb)
     e = rel_err(rm.accel, rp.accel)
     assert np.percentile(e, 99) < 2e-6
+
+
+def test_mixed_full_size_c2():
+    """The headline configuration at full size (N = 2^20 uniform cube, log-normal
+    masses, softening 1e-4, p = 10, theta 0.5, leaf 64), mixed form: p99 relative
+    force error against the FP64 direct sum on 1024 targets below 2e-6, and the
+    same interaction lists as the plain form."""
+    import fmms_b200 as fx
+
+    mass, pos = fx.gen_uniform_lognormal(1 << 20, 0.5, 22)
+    kw = dict(mac="theta", theta=0.5, softening=1e-4)
+    g = fx.Fmm(mass, pos, 10, 0.0, 64, precision="mixed", **kw)
+    res = g.run()
+    t = targets(len(mass), k=1024)
+    a_ref, _, _ = fx.direct_targets(mass, pos, t, softening=1e-4)
+    e = rel_err(res.accel[t], a_ref)
+    assert np.percentile(e, 99) < 2e-6, np.percentile(e, 99)
+    h = fx.Fmm(mass, pos, 10, 0.0, 64, **kw)
+    h.run()
+    for a, b in zip(g.export_lists(), h.export_lists()):
+        assert len(a) == len(b)
