@@ -44,6 +44,9 @@ __host__ __device__ constexpr int rot_moff(int k) { return 4 * (k * (k + 1) * (2
 #define ROTW_MAXP 16
 #define ROTW_MATS (rot_moff(ROTW_MAXP + 1))
 #define ROTW_NH (rot_hx(ROTW_MAXP, ROTW_MAXP) + 1)
+#ifndef ROTW_AXR_MAXP
+#define ROTW_AXR_MAXP 10
+#endif
 #define ROTW_LD 33  // entry stride of the per-lane columns (conflict-free both ways)
 
 static __constant__ ROTW_T c_rot[ROTW_MATS];            // P_k, Q_k, P_k^T, Q_k^T per degree
@@ -98,6 +101,22 @@ __device__ __forceinline__ void degree_fence() {
     if constexpr (sizeof(T) != 4 || P > 10) asm volatile("" ::: "memory");
 }
 
+// Where the back-rotated expansion b goes: the lane's shared-memory column,
+// from which the axial step reads it by order, or registers (FP32 at low
+// order), from which the forward rotation reads it directly.
+template <typename T>
+struct ColOut {
+    cplx<T>* col;
+    template <int E>
+    __device__ __forceinline__ void put(T re, T im) { col[ROTW_LD * E] = mk<T>(re, im); }
+};
+template <typename T, int H>
+struct RegOut {
+    T re[H], im[H];
+    template <int E>
+    __device__ __forceinline__ void put(T r, T i) { re[E] = r; im[E] = i; }
+};
+
 template <int M, typename T, int N>
 struct Unroll {  // compile-time loop helper: f(integral_constant<m>) for m = M..N-1
     template <class F>
@@ -131,8 +150,8 @@ __device__ __forceinline__ void swap_matvec(const T (&vr)[N], const T (&vi)[N], 
     });
 }
 
-template <typename T, int P, int K, bool FULL_LAYOUT, class PH>
-__device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa,
+template <typename T, int P, int K, bool FULL_LAYOUT, class PH, class OUT>
+__device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, const PH& ph_, OUT& out, T sa,
                                             T& sak, T cap) {
     typedef cplx<T> Z;
     constexpr int N = K + 1;
@@ -179,25 +198,25 @@ __device__ __forceinline__ void back_degree(const cplx<T>* __restrict__ ms, cons
         T orr = sr[r], oii = si[r];
         mul_i_pow<r>(orr, oii);
         const T g = c_ifm[rot_hx(K, r)] * sak;
-        col[ROTW_LD * rot_hx(K, r)] = mk<T>(orr * g, oii * g);
+        out.template put<rot_hx(K, r)>(orr * g, oii * g);
     });
     sak = min(sak * sa, cap);
     degree_fence<T, P>();
 }
 
-template <typename T, int P, bool FULL_LAYOUT, class PH, int... Ks>
-__device__ __forceinline__ void back_all(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa, T cap,
+template <typename T, int P, bool FULL_LAYOUT, class PH, class OUT, int... Ks>
+__device__ __forceinline__ void back_all(const cplx<T>* __restrict__ ms, const PH& ph_, OUT& out, T sa, T cap,
                                          std::integer_sequence<int, Ks...>) {
     T sak = T(1);
-    (back_degree<T, P, Ks, FULL_LAYOUT, PH>(ms, ph_, col, sa, sak, cap), ...);
+    (back_degree<T, P, Ks, FULL_LAYOUT, PH, OUT>(ms, ph_, out, sa, sak, cap), ...);
 }
 
 // `cap` bounds the scale powers of the normalised (mixed) form: a power only
 // exceeds 1 where the moments it multiplies are exactly zero (a cell of radius
 // 0), and the cap keeps that product 0 instead of 0 * inf.
-template <typename T, int P, bool FULL_LAYOUT, class PH>
-__device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, cplx<T>* col, T sa, T cap) {
-    back_all<T, P, FULL_LAYOUT, PH>(ms, ph_, col, sa, cap, std::make_integer_sequence<int, P + 1>{});
+template <typename T, int P, bool FULL_LAYOUT, class PH, class OUT>
+__device__ __forceinline__ void rotw_back(const cplx<T>* __restrict__ ms, const PH& ph_, OUT& out, T sa, T cap) {
+    back_all<T, P, FULL_LAYOUT, PH, OUT>(ms, ph_, out, sa, cap, std::make_integer_sequence<int, P + 1>{});
 }
 
 // axial translation of column m, in place:
@@ -240,20 +259,11 @@ __device__ __forceinline__ void rotw_axial(cplx<T>* col, T sb, T cap) {
     axial_all<T, P>(col, sb, cap, std::make_integer_sequence<int, P + 1>{});
 }
 
+// forward rotation of degree K from g = (-i)^m F / fm, result into the column
 template <typename T, int P, int K, class PH>
-__device__ __forceinline__ void fwd_degree(cplx<T>* col, const PH& ph_) {
+__device__ __forceinline__ void fwd_rotate(T (&vr)[K + 1], T (&vi)[K + 1], cplx<T>* col, const PH& ph_) {
     typedef cplx<T> Z;
     constexpr int N = K + 1;
-    T vr[N], vi[N];
-    Unroll<0, T, N>::run([&](auto mc) {  // g = (-i)^m F / fm
-        constexpr int m = decltype(mc)::value;
-        const Z F = col[ROTW_LD * rot_hx(K, m)];
-        T ur = F.re, ui = F.im;
-        mul_mi_pow<m>(ur, ui);
-        const T g = c_ifm[rot_hx(K, m)];
-        vr[m] = ur * g;
-        vi[m] = ui * g;
-    });
     T sr[N], si[N];
     swap_matvec<T, N, rot_moff(K) + 2 * N * N>(vr, vi, sr, si);
     Unroll<0, T, N>::run([&](auto rc) {  // q = conj(phb) * s
@@ -277,6 +287,58 @@ __device__ __forceinline__ void fwd_degree(cplx<T>* col, const PH& ph_) {
     degree_fence<T, P>();
 }
 
+template <typename T, int P, int K, class PH>
+__device__ __forceinline__ void fwd_degree(cplx<T>* col, const PH& ph_) {
+    typedef cplx<T> Z;
+    constexpr int N = K + 1;
+    T vr[N], vi[N];
+    Unroll<0, T, N>::run([&](auto mc) {  // g = (-i)^m F / fm
+        constexpr int m = decltype(mc)::value;
+        const Z F = col[ROTW_LD * rot_hx(K, m)];
+        T ur = F.re, ui = F.im;
+        mul_mi_pow<m>(ur, ui);
+        const T g = c_ifm[rot_hx(K, m)];
+        vr[m] = ur * g;
+        vi[m] = ui * g;
+    });
+    fwd_rotate<T, P, K, PH>(vr, vi, col, ph_);
+}
+
+// Axial translation fused into the forward rotation, b in registers: degree K
+// of the translated expansion is
+// F[K][m] = (-1)^m conj(sum_{k=m}^{P-K} b[k][m] (K+k)!) sb^{K+1}, formed right
+// where the forward rotation needs it (no shared-memory round trip).
+template <typename T, int P, int K, int H, class PH>
+__device__ __forceinline__ void axfwd_degree(const RegOut<T, H>& b, cplx<T>* col, const PH& ph_, T& sbn, T sb,
+                                             T cap) {
+    constexpr int N = K + 1;
+    T vr[N], vi[N];
+    Unroll<0, T, N>::run([&](auto mc) {  // g = (-i)^m F / fm
+        constexpr int m = decltype(mc)::value;
+        T ar = T(0), ai = T(0);
+        Unroll<m, T, P - K + 1>::run([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            ar += b.re[rot_hx(k, m)] * c_fact[K + k];
+            ai += b.im[rot_hx(k, m)] * c_fact[K + k];
+        });
+        constexpr T sg = (m & 1) ? T(-1) : T(1);
+        T ur = sg * ar * sbn, ui = -sg * ai * sbn;
+        mul_mi_pow<m>(ur, ui);
+        const T g = c_ifm[rot_hx(K, m)];
+        vr[m] = ur * g;
+        vi[m] = ui * g;
+    });
+    sbn = min(sbn * sb, cap);
+    fwd_rotate<T, P, K, PH>(vr, vi, col, ph_);
+}
+
+template <typename T, int P, int H, class PH, int... Ks>
+__device__ __forceinline__ void axfwd_all(const RegOut<T, H>& b, cplx<T>* col, const PH& ph_, T sb, T cap,
+                                          std::integer_sequence<int, Ks...>) {
+    T sbn = sb;
+    (axfwd_degree<T, P, Ks, H, PH>(b, col, ph_, sbn, sb, cap), ...);
+}
+
 template <typename T, int P, class PH, int... Ks>
 __device__ __forceinline__ void fwd_all(cplx<T>* col, const PH& ph_, std::integer_sequence<int, Ks...>) {
     (fwd_degree<T, P, Ks, PH>(col, ph_), ...);
@@ -293,7 +355,8 @@ __device__ __forceinline__ void rotw_fwd(cplx<T>* col, const PH& ph_) {
 template <typename T, int P, bool FULL_LAYOUT>
 __device__ __noinline__ void rotw_back_ni(const cplx<T>* __restrict__ ms, const cplx<T>* pa, const cplx<T>* pb,
                                           cplx<T>* col, T sa, T cap) {
-    rotw_back<T, P, FULL_LAYOUT>(ms, PhSmem<T>{pa, pb}, col, sa, cap);
+    ColOut<T> out{col};
+    rotw_back<T, P, FULL_LAYOUT>(ms, PhSmem<T>{pa, pb}, out, sa, cap);
 }
 template <typename T, int P>
 __device__ __noinline__ void rotw_axial_ni(cplx<T>* col, T sb, T cap) {
@@ -314,6 +377,8 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
     constexpr int DIM = (P + 1) * (P + 1);
     typedef cplx<T> Z;
     constexpr bool PH_REGS = sizeof(T) == 4;
+    // FP32 up to ROTW_AXR_MAXP: b stays in registers through the axial step
+    constexpr bool AXR = PH_REGS && P <= ROTW_AXR_MAXP;
     Z* col = sbuf + lane;                    // this lane's column: entry e at col[LD e]
     Z* pha = sbuf + ROTW_LD * H + lane;      // e^{imα}, m = 0..P (FP64 only)
     Z* phb = pha + ROTW_LD * (P + 1);        // e^{imβ}
@@ -365,8 +430,13 @@ __device__ __forceinline__ void rotw_body(int c, uint32_t beg, uint32_t end, con
             }
             const Z* ms = mom + (size_t)src * (FULL_LAYOUT ? DIM : half_stride(P));
             const T cap = SCALED ? T(1e30) : T(INFINITY);
-            if constexpr (PH_REGS) {
-                rotw_back<T, P, FULL_LAYOUT>(ms, phr, col, sa, cap);
+            if constexpr (AXR) {
+                RegOut<T, H> b;
+                rotw_back<T, P, FULL_LAYOUT>(ms, phr, b, sa, cap);
+                axfwd_all<T, P, H>(b, col, phr, sb, cap, std::make_integer_sequence<int, P + 1>{});
+            } else if constexpr (PH_REGS) {
+                ColOut<T> out{col};
+                rotw_back<T, P, FULL_LAYOUT>(ms, phr, out, sa, cap);
                 rotw_axial<T, P>(col, sb, cap);
                 rotw_fwd<T, P>(col, phr);
             } else {
