@@ -469,7 +469,7 @@ def run_graphs(args, cfg, rank, world, local_rank):
     mass, pos = make_inputs(fx, cfg)
     n = len(mass)
     vel = np.zeros_like(pos)
-    refresh = max(args.refresh_every, 2)
+    refresh = args.refresh_every if args.refresh_every > 1 else 8
     res = {}
     side = torch.cuda.Stream(device=dev)
     with torch.cuda.stream(side):

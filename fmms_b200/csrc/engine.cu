@@ -1103,6 +1103,8 @@ fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const doubl
     return evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot);
 }
 
+static constexpr int kGraphMinUses = 2;
+
 fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, const double* d_mass, double* d_acc,
                                  double* d_pot, double dt, int nsteps, int scheme, int refresh_every) {
     if (!ctx) return FMMX_INVALID_ARG;
@@ -1123,9 +1125,14 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, co
         // A step on a reused tree is the same sequence of launches every time:
         // record it once as a CUDA graph and replay it (one launch instead of
         // about 30). Not on the legacy default stream, which cannot be captured.
-        if (!rebuild && ctx->cfg.use_graphs && s != nullptr && ctx->lists_valid) {
-            const bool same = ctx->step_graph && ctx->graph_dt == dt && ctx->graph_scheme == scheme &&
-                              std::equal(key, key + 5, ctx->graph_key);
+        // A recording costs more than a launched step, so a tree is recorded
+        // only when the refresh cadence will replay it at least
+        // kGraphMinUses times (steps_since_build counts the reuse steps done).
+        const bool same = ctx->step_graph && ctx->graph_dt == dt && ctx->graph_scheme == scheme &&
+                          std::equal(key, key + 5, ctx->graph_key);
+        const int reuse_left = refresh_every - 1 - ctx->steps_since_build;
+        if (!rebuild && ctx->cfg.use_graphs && s != nullptr && ctx->lists_valid &&
+            (same || reuse_left >= kGraphMinUses)) {
             if (!same) {
                 ctx->drop_graph();
                 const bool ev_saved = ctx->events;
