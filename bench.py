@@ -666,7 +666,7 @@ def run_serve(args, cfg, rank, world, local_rank):
     Plummer or uniform-cube sessions (50/50), N log-uniform in [1e3, 1e6], 100
     KDK steps of dt = 1e-3 each, admitted under the HBM budget."""
     import fmms_b200 as fx
-    from fmms_b200.serve import Server, Session, run_session_alone
+    from fmms_b200.serve import Server, Session, run_session_alone, worst_intervals
 
     if rank != 0:
         return
@@ -727,7 +727,7 @@ def run_serve(args, cfg, rank, world, local_rank):
                       "admitted_sessions_mean": float(np.mean([o[0] for o in occ])) if occ else 0.0,
                       "admitted_bodies_mean": float(np.mean([o[1] for o in occ])) if occ else 0.0,
                       "lanes": [{"n_from": ln.lo, "stream_priority": ln.priority, "ticks": len(ln.tick_ms),
-                                 "joins_undone": ln.evictions,
+                                 "joins_undone": ln.evictions, "worst_intervals": worst_intervals(ln.trace, copies=srv.copy_log),
                                  "tick_ms_p50": float(np.percentile(ln.tick_ms, 50)) if ln.tick_ms else None}
                                 for ln in srv.lanes],
                       "p99_over_isolated": {"median": float(np.median(rr)) if rr else None,

@@ -13,11 +13,15 @@ evaluation with a zero time step (that evaluation gives its initial forces, so
 joining costs the others no extra pass), steps from the tick after, and leaves
 (freeing its memory) at the end of the tick that finishes it.
 
-Host<->device traffic stays off the step path: a submitted session's bodies are
-staged to the device on a copy stream by the submitting thread while it waits,
-and a finished session's final state is copied back to the host by a collector
-thread (in synchronous mode by `Server.collect`) while the lane goes on with
-its next tick.
+Host<->device traffic stays off the step path and on the thread that issues
+every other CUDA call: submitting a session only queues it. After a tick's
+launches, while the device runs that tick, the first lane's thread moves
+queued bodies to the device and finished sessions' final states to the host
+in slices of a few MB (`Server.pump`, bounded by half the tick's expected
+device time), through page-locked buffers allocated once (`PinnedRing`) on a
+copy stream. Copies issued from other host threads at the same time as a
+lane's launches (pageable or pinned) held those launches up for tens to
+hundreds of milliseconds on the B200 boxes measured.
 
 Latency: a session's step latency is the wall-clock interval between the ends
 of its consecutive steps; every step should take at most `latency_slo` times
@@ -67,6 +71,7 @@ RESIDENT_BYTES_PER_BODY = 96
 ENGINE_BYTES_PER_BODY = 640
 SESSION_FIXED_BYTES = 1 << 20
 STAGED_BYTES_PER_BODY = 56  # pos, vel, mass staged on the device while queued
+SMALL_POOL_RESERVE = 256 << 20  # small-block pool reserved per stream (blocks <= 1 MB)
 
 # Size classes (lower bounds of N) of the lanes: one lane by default.
 LANE_BOUNDS = (0,)
@@ -95,7 +100,8 @@ class Session:
     result_pos: np.ndarray | None = None
     result_vel: np.ndarray | None = None
     staged: tuple | None = dataclasses.field(default=None, repr=False)  # device pos, vel, mass, ready event
-    pending: tuple | None = dataclasses.field(default=None, repr=False)  # device pos, vel copies, ready event
+    pending: tuple | None = dataclasses.field(default=None, repr=False)  # result copy job, host pos, host vel
+    stage_job: object | None = dataclasses.field(default=None, repr=False)  # staging in progress
 
     @property
     def n(self) -> int:
@@ -108,7 +114,7 @@ class Session:
         """The same request, not yet served."""
         return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
                                    primed=False, last_end=0.0, retry_after=-1, step_ms=[], result_pos=None,
-                                   result_vel=None, staged=None, pending=None)
+                                   result_vel=None, staged=None, pending=None, stage_job=None)
 
 
 def _interp_loglog(ns, vals, n):
@@ -119,6 +125,85 @@ def _interp_loglog(ns, vals, n):
         slope = max((lv[-1] - lv[-2]) / (ln[-1] - ln[-2]), 0.0)
         return float(np.exp(lv[-1] + slope * (x - ln[-1])))
     return float(np.exp(np.interp(x, ln, lv)))
+
+
+class CopyJob:
+    """A host<->device copy done in chunks: parts of (host uint8 view, device
+    uint8 view), all in one direction."""
+
+    def __init__(self, parts, to_device: bool):
+        self.parts = [(h, d) for h, d in parts if h.size > 0]
+        self.to_device = to_device
+        self.i = 0
+        self.off = 0
+        self.lock = threading.Lock()
+
+    @property
+    def done(self) -> bool:
+        return self.i >= len(self.parts)
+
+
+class PinnedRing:
+    """Page-locked host buffers, allocated once, through which copy jobs move
+    chunk by chunk on a given stream: host-to-device double-buffered (the host
+    fills one buffer while the other's DMA runs), device-to-host one chunk at
+    a time."""
+
+    def __init__(self, torch, chunk_bytes=4 << 20):
+        self.torch = torch
+        self.chunk = int(chunk_bytes)
+        self.up = [torch.empty(self.chunk, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+        self.up_np = [b.numpy() for b in self.up]
+        self.up_ev = [None, None]
+        self.up_next = 0
+        self.down = torch.empty(self.chunk, dtype=torch.uint8, pin_memory=True)
+        self.down_np = self.down.numpy()
+        self.lock = threading.Lock()
+
+    def advance(self, job: CopyJob, stream) -> bool:
+        """Move one chunk of `job` on `stream`; True once the job is complete
+        (host-to-device: queued on the stream; device-to-host: on the host)."""
+        torch = self.torch
+        with job.lock, self.lock, torch.cuda.stream(stream):
+            if job.done:
+                return True
+            h, d = job.parts[job.i]
+            m = min(self.chunk, h.size - job.off)
+            sl = slice(job.off, job.off + m)
+            if job.to_device:
+                k = self.up_next
+                self.up_next ^= 1
+                if self.up_ev[k] is not None:
+                    self.up_ev[k].synchronize()  # this buffer's previous DMA is done
+                np.copyto(self.up_np[k][:m], h[sl])
+                d[sl].copy_(self.up[k][:m], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                self.up_ev[k] = ev
+            else:
+                self.down[:m].copy_(d[sl], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                ev.synchronize()
+                np.copyto(h[sl], self.down_np[:m])
+            job.off += m
+            if job.off >= h.size:
+                job.i += 1
+                job.off = 0
+            return job.done
+
+    def finish(self, job: CopyJob, stream):
+        while not self.advance(job, stream):
+            pass
+
+
+def _u8(a):
+    """uint8 view of a contiguous host array or device tensor."""
+    if isinstance(a, np.ndarray):
+        return a.reshape(-1).view(np.uint8)
+    import torch
+
+    return a.reshape(-1).view(torch.uint8)
 
 
 class LatencyModel:
@@ -139,6 +224,41 @@ class LatencyModel:
 
     def table(self):
         return [[n, round(a, 3), round(b, 3)] for n, a, b in zip(self.ns, self.iso_ms, self.extra_ms)]
+
+
+# Fields of a lane's per-tick trace record: perf_counter seconds at the tick's
+# start, after admission and joins, after the step's launches, after the device
+# finished it, and at the tick's end (departures done); then its device time
+# (ms), members, bodies, sessions joined, joins undone and departures; then the
+# times inside the launch phase after the first kick and drift, after the
+# forest build and after the evaluation.
+TICK_FIELDS = ("t_start", "t_joined", "t_launched", "t_synced", "t_end", "device_ms", "members", "bodies",
+               "joined", "undone", "left", "t_kick_drift", "t_built", "t_evaluated")
+
+
+def worst_intervals(trace, k=8, copies=()):
+    """The k longest intervals between consecutive tick ends of a lane, each
+    split into its host phases: idle gap before the tick, admission and joins,
+    launches, wait for the device, departures (ms); with `copies` (a server's
+    copy log), the staging and result copy time that overlapped the interval."""
+    out = []
+    tr = list(trace)
+    cp = list(copies)
+    for a, b in zip(tr, tr[1:]):
+        out.append({"interval_ms": 1e3 * (b[4] - a[4]), "gap_ms": 1e3 * (b[0] - a[4]), "join_ms": 1e3 * (b[1] - b[0]),
+                    "launch_ms": 1e3 * (b[2] - b[1]), "sync_ms": 1e3 * (b[3] - b[2]), "leave_ms": 1e3 * (b[4] - b[3]),
+                    "device_ms": b[5], "members": b[6], "bodies": b[7], "joined": b[8], "undone": b[9],
+                    "left": b[10], "_t": (a[4], b[4]), "kick_drift_ms": 1e3 * (b[11] - b[1]),
+                    "build_ms": 1e3 * (b[12] - b[11]), "evaluate_ms": 1e3 * (b[13] - b[12]),
+                    "last_kick_ms": 1e3 * (b[2] - b[13])})
+    out.sort(key=lambda r: -r["interval_ms"])
+    out = out[:k]
+    for r in out:
+        t0, t1 = r.pop("_t")
+        r["copy_overlap_ms"] = 1e3 * sum(max(0.0, min(c[1], t1) - max(c[0], t0)) for c in cp)
+        r["copies"] = [[c[2], round(1e3 * (c[0] - t0), 2), round(1e3 * (c[1] - c[0]), 2), round(c[3] / 1e6, 2)]
+                       for c in cp if c[1] > t0 and c[0] < t1][:12]
+    return [{k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in r.items()} for r in out[:k]]
 
 
 class Lane:
@@ -165,6 +285,9 @@ class Lane:
         self.bodies_stepped = 0
         self.departures = 0  # sessions finished in this lane
         self.evictions = 0  # joins undone because the joining tick broke the bound
+        self.t_built = 0.0
+        # one record per tick (TickRecord fields), for latency analysis
+        self.trace: deque[tuple] = deque(maxlen=1 << 17)
 
     # ---------------------------------------------------------------- helpers
     @staticmethod
@@ -180,6 +303,7 @@ class Lane:
 
     def evaluate(self, pos, mass, acc, pot, offsets):
         self.fmm.build_ensemble_device(offsets, pos.data_ptr(), mass.data_ptr())
+        self.t_built = time.perf_counter()
         self.fmm.evaluate_device(pos.data_ptr(), mass.data_ptr(), acc.data_ptr(), pot.data_ptr())
 
     # ---------------------------------------------------------------- admission
@@ -219,7 +343,7 @@ class Lane:
         torch = self.srv.torch
         for s in new:
             if s.staged is None:
-                self.srv.stage(s)
+                self.srv.stage_now(s)
             self.stream.wait_event(s.staged[3])
         pos = torch.cat([s.staged[0] for s in new])
         vel = torch.cat([s.staged[1] for s in new])
@@ -283,7 +407,9 @@ class Lane:
         for s, p, v in out:
             ev = torch.cuda.Event()
             ev.record(self.stream)
-            s.pending = (p, v, ev)
+            self.srv.copy_stream.wait_event(ev)  # the copies read what this tick wrote
+            hp, hv = np.empty((s.n, 3)), np.empty((s.n, 3))
+            s.pending = (CopyJob([(_u8(hp), _u8(p)), (_u8(hv), _u8(v))], to_device=False), hp, hv)
             s.finished_at = now
             self.srv.release(s.bytes_needed())
             self.srv.finished(s)
@@ -306,9 +432,11 @@ class Lane:
         torch = self.srv.torch
         t_start = time.perf_counter()
         with torch.cuda.stream(self.stream):
-            self.join(self.admit(time.perf_counter()))
+            new = self.admit(time.perf_counter())
+            self.join(new)
             if not self.members:
                 return 0.0
+            t_joined = time.perf_counter()
             stepping = self.stepping
             pos, vel, acc, pot, mass = self.state
             e0 = torch.cuda.Event(enable_timing=True)
@@ -317,13 +445,21 @@ class Lane:
             if stepping:
                 vel.add_(0.5 * self.dts * acc)
                 pos.add_(self.dts * vel)
+            t_kd = time.perf_counter()
             self.evaluate(pos, mass, acc, pot, self.offsets(self.members))
+            t_ev = time.perf_counter()
             if stepping:
                 vel.add_(0.5 * self.dts * acc)
+            t_launched = time.perf_counter()
             e1.record(self.stream)
+            if self.srv.lanes[0] is self:
+                # copies in the shadow of this tick's device time
+                expect = self.tick_ms[-1] if self.tick_ms else 1.0
+                self.srv.pump(0.5e-3 * expect)
             e1.synchronize()
             t_end = time.perf_counter()
             ms = e0.elapsed_time(e1)
+            n_members, n_bodies, ev0, dep0 = len(self.members), self.bodies(), self.evictions, self.departures
             self.tick_ms.append(ms)
             for s in stepping:
                 s.steps_done += 1
@@ -354,6 +490,8 @@ class Lane:
             changed = self.leave(time.perf_counter())
             if joined or changed:
                 self._set_dts()
+            self.trace.append((t_start, t_joined, t_launched, t_end, time.perf_counter(), ms, n_members, n_bodies,
+                               len(new), self.evictions - ev0, self.departures - dep0, t_kd, self.t_built, t_ev))
             return ms
 
 
@@ -370,7 +508,7 @@ class Server:
 
     def __init__(self, *, p=8, theta=0.5, softening=1e-3, n_leaf=64, precision="mixed", budget_bytes=160e9,
                  lanes=LANE_BOUNDS, device=0, latency_slo=None, headroom=None, model=None, max_bypass_s=2.0,
-                 scan=256, stage_limit_bytes=8e9):
+                 scan=256, stage_limit_bytes=8e9, lane_reserve_bytes=2e9):
         import torch
 
         import fmms_b200 as fx
@@ -391,6 +529,13 @@ class Server:
         self.max_bypass_s = max_bypass_s
         self.scan = scan
         self.copy_stream = torch.cuda.Stream(device=device)
+        self.ring = PinnedRing(torch)
+        self.copy_lock = threading.RLock()  # one copy activity at a time (several lanes may join)
+        self.to_stage: deque[Session] = deque()  # submitted, not staged, within the staging limit
+        self.staging: Session | None = None  # the session being staged
+        self.results: deque[Session] = deque()  # finished, final state still to copy
+        # (start, end, kind, bytes) of every staging and result copy, perf_counter seconds
+        self.copy_log: deque[tuple] = deque(maxlen=1 << 16)
         bounds = tuple(sorted(lanes))
         try:
             least, greatest = torch.cuda.Stream.priority_range()
@@ -401,6 +546,19 @@ class Server:
             prio = max(greatest, least - (len(bounds) - 1 - i)) if greatest < least else least
             # with several lanes, short M2L blocks let the higher-priority lanes in
             self.lanes.append(Lane(self, lo, prio, preemptible=len(bounds) > 1))
+        # Device allocations in the steady state come from the caching
+        # allocator's pools, one per stream and size class (blocks up to 1 MB
+        # are carved from 2 MB segments, larger ones from their own): reserve
+        # both up front (allocate and free once), so that staging, joins and
+        # kicks do not reach cudaMalloc, which was seen to take ~90 ms at times
+        # on a busy device, even for a 2 MB segment.
+        for st, nbytes in [(self.copy_stream, self.stage_limit)] + [(ln.stream, lane_reserve_bytes) for ln in self.lanes]:
+            if nbytes > 0:
+                with torch.cuda.stream(st):
+                    blk = torch.empty(int(nbytes), dtype=torch.uint8, device=self.dev)
+                    small = [torch.empty(1 << 20, dtype=torch.uint8, device=self.dev)
+                             for _ in range(int(min(nbytes, SMALL_POOL_RESERVE)) >> 20)]
+                    del blk, small
         self.done: list[Session] = []
         self.outstanding = 0
         self._threads = []
@@ -450,6 +608,7 @@ class Server:
             extra.append(max(ext_t))
         for ln in self.lanes:
             ln.tick_ms.clear()
+            ln.trace.clear()
             ln.bodies_stepped = 0
         return LatencyModel(ns, iso, extra)
 
@@ -468,41 +627,110 @@ class Server:
     def mem_used(self) -> float:
         return self.used
 
-    def stage(self, s: Session):
-        """Bodies of a waiting session to the device on the copy stream (the
-        calling thread waits for the copy; no pinned allocations); the copy's
-        event orders their use on a lane's stream."""
+    def _start_staging(self, s: Session):
         torch = self.torch
+        t0 = time.perf_counter()
         with torch.cuda.stream(self.copy_stream):
-            dev = [torch.from_numpy(np.ascontiguousarray(a)).to(self.dev) for a in (s.pos, s.vel, s.mass)]
-            ev = torch.cuda.Event()
-            ev.record(self.copy_stream)
+            dev = [torch.empty(tuple(np.shape(a)), dtype=torch.float64, device=self.dev) for a in (s.pos, s.vel, s.mass)]
+        self.copy_log.append((t0, time.perf_counter(), "alloc", s.n * STAGED_BYTES_PER_BODY))
+        host = [_u8(np.ascontiguousarray(a, dtype=np.float64)) for a in (s.pos, s.vel, s.mass)]
+        s.stage_job = (CopyJob([(h, _u8(d)) for h, d in zip(host, dev)], to_device=True), dev, time.perf_counter())
+
+    def _end_staging(self, s: Session):
+        torch = self.torch
+        job, dev, t0 = s.stage_job
+        ev = torch.cuda.Event()
+        ev.record(self.copy_stream)
         s.staged = (dev[0], dev[1], dev[2], ev)
+        s.stage_job = None
+        self.copy_log.append((t0, time.perf_counter(), "stage", s.n * STAGED_BYTES_PER_BODY))
+
+    def stage_now(self, s: Session):
+        """Stage a joining session's bodies completely (it was not staged in
+        the background, or only in part)."""
+        with self.copy_lock:
+            self._stage_now(s)
+
+    def _stage_now(self, s: Session):
         with self.lock:
-            self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+            if self.staging is s:
+                self.staging = None
+            elif s in self.to_stage:
+                self.to_stage.remove(s)
+            else:
+                self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+        if s.stage_job is None:
+            self._start_staging(s)
+        self.ring.finish(s.stage_job[0], self.copy_stream)
+        self._end_staging(s)
 
     def unstage(self, n_bodies):
         with self.lock:
             self.staged_bytes -= n_bodies * STAGED_BYTES_PER_BODY
 
+    def pump(self, budget_s: float) -> bool:
+        """Result copies first, then staging, one chunk at a time, for about
+        `budget_s` seconds (at least one chunk when there is work); False if
+        there was nothing to copy."""
+        t_end = time.perf_counter() + budget_s
+        while True:
+            with self.copy_lock:
+                if not self._pump_one():
+                    return False
+            if time.perf_counter() >= t_end:
+                return True
+
+    def _pump_one(self) -> bool:
+        """One chunk of the oldest result copy, else of the staging in
+        progress (starting the next one if none is); False if idle."""
+        if self.results:
+            s = self.results[0]
+            if self.ring.advance(s.pending[0], self.copy_stream):
+                self._finish_result(s)
+            return True
+        with self.lock:
+            s = self.staging
+            if s is None and self.to_stage:
+                s = self.staging = self.to_stage.popleft()
+        if s is None:
+            return False
+        if s.staged is None:
+            if s.stage_job is None:
+                self._start_staging(s)
+            if not self.ring.advance(s.stage_job[0], self.copy_stream):
+                return True
+            self._end_staging(s)
+        with self.lock:
+            if self.staging is s:
+                self.staging = None
+        return True
+
+    def _finish_result(self, s: Session):
+        job, hp, hv = s.pending
+        s.result_pos, s.result_vel = hp, hv
+        s.pending = None
+        if self.results and self.results[0] is s:
+            self.results.popleft()
+        self.copy_log.append((s.finished_at, time.perf_counter(), "collect", 48 * s.n))
+
     def collect(self, sessions=None):
-        """Copy the final state of finished sessions to the host (on the copy
-        stream, after the lane's stream produced it) and fill their results."""
-        torch = self.torch
-        for s in list(self.done if sessions is None else sessions):
-            pend = s.pending
-            if pend is None:
-                continue
-            p, v, ev = pend
-            self.copy_stream.wait_event(ev)
-            with torch.cuda.stream(self.copy_stream):
-                s.result_pos = p.cpu().numpy()
-                s.result_vel = v.cpu().numpy()
-            s.pending = None
+        """Finish the final-state copies of finished sessions (all of them, or
+        of `sessions`)."""
+        with self.copy_lock:
+            self._collect(sessions)
+
+    def _collect(self, sessions):
+        for s in list(self.results if sessions is None else sessions):
+            if s.pending is not None:
+                self.ring.finish(s.pending[0], self.copy_stream)
+                self._finish_result(s)
+                if s in self.results:
+                    self.results.remove(s)
 
     def finished(self, s):
         with self.lock:
             self.done.append(s)
+            self.results.append(s)
             self.outstanding -= 1
 
     def busy(self) -> bool:
@@ -524,10 +752,12 @@ class Server:
         return lane
 
     def submit(self, s: Session, lane=None):
+        """Queue a session (any thread; no CUDA call here)."""
         s.submitted_at = time.perf_counter()
-        if self.staged_bytes + s.n * STAGED_BYTES_PER_BODY <= self.stage_limit:
-            self.stage(s)
         with self.lock:
+            if self.staged_bytes + s.n * STAGED_BYTES_PER_BODY <= self.stage_limit:
+                self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+                self.to_stage.append(s)
             self.outstanding += 1
             (lane or self.lane_for(s)).queue.append(s)
 
@@ -550,6 +780,8 @@ class Server:
         t = 0
         while self.busy() and t < max_ticks:
             self.tick()
+            if not any(ln.members for ln in self.lanes):
+                self.pump(0.001)  # admission waits on staging: keep it moving
             t += 1
         self.collect()
 
@@ -561,14 +793,9 @@ class Server:
             while not self._stop.is_set():
                 if ln.members or ln.queue:
                     ln.tick()
-                if not ln.members:  # idle, or admission refused: do not spin on the GIL
-                    time.sleep(0.0005)
-
-        def collector():
-            self.torch.cuda.set_device(self.device)
-            while not self._stop.is_set():
-                self.collect()
-                time.sleep(0.005)
+                if not ln.members:  # idle, or admission refused: copy, else do not spin on the GIL
+                    if not (ln is self.lanes[0] and self.pump(0.001)):
+                        time.sleep(0.0005)
 
         # lane threads hand the interpreter lock to each other and to the
         # submitting thread between short pieces of host work; the default 5 ms
@@ -579,9 +806,6 @@ class Server:
             th = threading.Thread(target=loop, args=(ln,), daemon=True)
             th.start()
             self._threads.append(th)
-        th = threading.Thread(target=collector, daemon=True)
-        th.start()
-        self._threads.append(th)
 
     def stop(self):
         self._stop.set()
@@ -617,6 +841,8 @@ class Server:
 def run_session_alone(sess: Session, **kw) -> tuple[np.ndarray, np.ndarray, list]:
     """The same session through its own server, for alone-vs-mix checks."""
     kw = {k: v for k, v in kw.items() if k not in ("latency_slo", "headroom", "model")}
+    kw.setdefault("stage_limit_bytes", 0)  # one session: staged when it joins, no pools reserved
+    kw.setdefault("lane_reserve_bytes", 0)
     srv = Server(**kw)
     srv.submit(sess.fresh())
     srv.run_until_idle()
