@@ -504,6 +504,10 @@ class Server:
     under the HBM budget only).
     headroom: the bound used for admission decisions (below latency_slo, to
     leave room for prediction error).
+    stage_limit_bytes: device bytes of queued sessions' bodies staged ahead of
+    their admission (sessions beyond it are staged when they join); also the
+    allocator pool reserved on the copy stream.
+    lane_reserve_bytes: allocator pool reserved on each lane's stream.
     """
 
     def __init__(self, *, p=8, theta=0.5, softening=1e-3, n_leaf=64, precision="mixed", budget_bytes=160e9,
