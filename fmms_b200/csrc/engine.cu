@@ -39,12 +39,16 @@ struct DBuf {
     }
     // Grows by at least half of the current capacity, so a context that sees
     // slowly growing inputs (a serving loop's forests) reallocates -- and
-    // cudaFree synchronises the device -- only a logarithmic number of times.
+    // cudaFree synchronises the device -- only a logarithmic number of times;
+    // a first allocation carries 1/8 slack, so that sizes which drift up a
+    // little between calls (a leapfrog's interaction lists) do not reallocate
+    // at the first step (cudaMalloc of a large buffer took over a second at
+    // times on a busy device).
     cudaError_t ensure(size_t n) {
         if (n <= cap && p) return cudaSuccess;
         const size_t grown = cap + cap / 2;
         release();
-        size_t want = std::max<size_t>(std::max<size_t>(n, grown), 1);
+        size_t want = std::max<size_t>(std::max<size_t>(n + n / 8, grown), 1);
         cudaError_t e = cudaMalloc((void**)&p, want * sizeof(T));
         if (e != cudaSuccess && want > n) {  // no room for the slack: exactly n
             cudaGetLastError();
