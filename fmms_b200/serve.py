@@ -568,6 +568,7 @@ class Server:
         self._threads = []
         self._stop = threading.Event()
         self._switch = None
+        self.error: BaseException | None = None  # first exception of a lane thread
         self.model = None
         if latency_slo is not None:
             self.model = model if model is not None else self.calibrate()
@@ -738,8 +739,9 @@ class Server:
             self.outstanding -= 1
 
     def busy(self) -> bool:
-        """Sessions submitted and not finished (queued, joining or stepping)."""
-        return self.outstanding > 0
+        """Sessions submitted and not finished (queued, joining or stepping);
+        False once a lane thread has failed (`stop` raises its exception)."""
+        return self.outstanding > 0 and self.error is None
 
     def gate_open(self, lane) -> bool:
         """Admission feedback: the lane's recent steps within the headroom."""
@@ -793,13 +795,19 @@ class Server:
         """Threaded mode: every lane ticks on its own host thread and stream."""
 
         def loop(ln):
-            self.torch.cuda.set_device(self.device)
-            while not self._stop.is_set():
-                if ln.members or ln.queue:
-                    ln.tick()
-                if not ln.members:  # idle, or admission refused: copy, else do not spin on the GIL
-                    if not (ln is self.lanes[0] and self.pump(0.001)):
-                        time.sleep(0.0005)
+            try:
+                self.torch.cuda.set_device(self.device)
+                while not self._stop.is_set():
+                    if ln.members or ln.queue:
+                        ln.tick()
+                    if not ln.members:  # idle, or admission refused: copy, else do not spin on the GIL
+                        if not (ln is self.lanes[0] and self.pump(0.001)):
+                            time.sleep(0.0005)
+            except BaseException as e:  # noqa: BLE001 - handed to the caller by stop()
+                with self.lock:
+                    if self.error is None:
+                        self.error = e
+                self._stop.set()  # the other lanes stop too
 
         # lane threads hand the interpreter lock to each other and to the
         # submitting thread between short pieces of host work; the default 5 ms
@@ -812,6 +820,8 @@ class Server:
             self._threads.append(th)
 
     def stop(self):
+        """Stop the lane threads and finish the result copies; raises the
+        first exception a lane thread met, if any."""
         self._stop.set()
         for th in self._threads:
             th.join()
@@ -820,6 +830,8 @@ class Server:
         if self._switch is not None:
             sys.setswitchinterval(self._switch)
             self._switch = None
+        if self.error is not None:
+            raise RuntimeError("serving lane failed") from self.error
         self.collect()
 
     def report(self) -> dict:
