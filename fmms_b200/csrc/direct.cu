@@ -202,14 +202,21 @@ extern "C" fmmx_status fmmx_direct_targets_noalloc(int device, void* stream, siz
         }
         scratch = g_scratch_addr[device];
     }
+    // an error left by earlier, unrelated work on this thread is not this
+    // call's: report it without launching and leave it for its owner (peek,
+    // do not clear); after that, an error is one of the launches below
+    if (st == FMMX_OK && cudaPeekAtLastError() != cudaSuccess) st = FMMX_DEVICE_ERROR;
     if (st == FMMX_OK) {
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         dim3 g((unsigned)((nt + DIR_BLOCK - 1) / DIR_BLOCK), FMMX_NOALLOC_NSPLIT);
         fmmx::k_direct_targets_checked<<<g, DIR_BLOCK, 0, s>>>(d_pos, d_mass, n, d_targets, nt,
                                                                softening * softening, scratch);
-        fmmx::k_direct_reduce<<<fmmx::grid_for(nt, 128), 128, 0, s>>>(scratch, FMMX_NOALLOC_NSPLIT, nt, d_acc, d_pot,
-                                                                      d_fscale);
         if (cudaGetLastError() != cudaSuccess) st = FMMX_DEVICE_ERROR;
+        if (st == FMMX_OK) {
+            fmmx::k_direct_reduce<<<fmmx::grid_for(nt, 128), 128, 0, s>>>(scratch, FMMX_NOALLOC_NSPLIT, nt, d_acc,
+                                                                          d_pot, d_fscale);
+            if (cudaGetLastError() != cudaSuccess) st = FMMX_DEVICE_ERROR;
+        }
     }
     cudaSetDevice(prev);
     return st;

@@ -807,6 +807,10 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     }
     if (tm) CK(cudaEventRecord(ev[10], s2), "event");
     if (!reuse) {
+        // a recorded leapfrog step addresses the list buffers and list sizes of
+        // the last walk; this walk and its lists may reallocate or resize them
+        ctx->drop_graph();
+        ctx->lists_valid = false;
         fmmx_status st = walk_impl(ctx, s2);
         if (st != FMMX_OK) return st;
         if (dehnen) {

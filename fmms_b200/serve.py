@@ -820,8 +820,11 @@ class Server:
             self._threads.append(th)
 
     def stop(self):
-        """Stop the lane threads and finish the result copies; raises the
-        first exception a lane thread met, if any."""
+        """Stop the lane threads and finish the result copies of the sessions
+        that completed; then raise the first exception a lane thread met, if
+        any. The error is cleared as it is raised, so the server can be
+        started again (sessions that were active on the failed lane stay in
+        ``active`` and are not resumed)."""
         self._stop.set()
         for th in self._threads:
             th.join()
@@ -830,9 +833,12 @@ class Server:
         if self._switch is not None:
             sys.setswitchinterval(self._switch)
             self._switch = None
-        if self.error is not None:
-            raise RuntimeError("serving lane failed") from self.error
-        self.collect()
+        err, self.error = self.error, None
+        try:
+            self.collect()
+        finally:
+            if err is not None:
+                raise RuntimeError("serving lane failed") from err
 
     def report(self) -> dict:
         sess = self.done + self.active

@@ -46,6 +46,9 @@ def lib():
         L.orc_plummer.argtypes = [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]
         L.orc_hernquist.argtypes = [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp]
         L.orc_rng_units.argtypes = [C.c_uint64, _sz, _dp]
+        L.orc_gen_plummer_ic.argtypes = [_sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp, _dp, _dp]
+        L.orc_gen_uniform_lognormal.argtypes = [_sz, C.c_double, C.c_uint64, _dp, _dp]
+        L.orc_gen_clusters.argtypes = [_sz, C.c_int, C.c_double, C.c_double, C.c_uint64, _dp, _dp, _dp]
         L.orc_theta_table.argtypes = [_dp, _sz, _dp]
         L.orc_upsilon_table.argtypes = [_dp, _sz, _dp]
         L.orc_dilate.argtypes = [C.c_uint64]
@@ -61,6 +64,7 @@ def lib():
         L.orc_fmm_free.argtypes = [C.c_void_p]
         L.orc_fmm_set_gap.argtypes = [C.c_void_p, C.c_double]
         L.orc_fmm_run.argtypes = [C.c_void_p, _sz, _dp, _dp, C.c_int, _dp, _dp]
+        L.orc_fmm_walk.argtypes = [C.c_void_p, _sz, _dp, _dp, C.c_int]
         L.orc_fmm_ncells.argtypes = [C.c_void_p]
         L.orc_fmm_ncells.restype = _sz
         L.orc_fmm_cells.argtypes = [C.c_void_p, _u32p, _i32p, _dp, _dp, _dp]
@@ -110,6 +114,30 @@ def hernquist(n: int, center=(0.0, 0.0, 0.0), seed: int = 7):
     pos = np.empty((n, 3))
     lib().orc_hernquist(n, center[0], center[1], center[2], seed, _ptr(mass, _dp), _ptr(pos, _dp))
     return mass, pos
+
+
+def gen_plummer_ic(n, mtot=1.0, a=1.0, rmax=20.0, seed=1, velocities=True):
+    """Benchmark workload (no reference counterpart): Plummer sphere truncated
+    at r <= rmax*a with distribution-function velocities -> (mass, pos, vel)."""
+    mass, pos = np.empty(n), np.empty((n, 3))
+    vel = np.empty((n, 3)) if velocities else None
+    lib().orc_gen_plummer_ic(n, mtot, a, rmax, seed, _ptr(mass, _dp), _ptr(pos, _dp), _ptr(vel, _dp))
+    return mass, pos, vel
+
+
+def gen_uniform_lognormal(n, sigma=0.5, seed=2):
+    """Benchmark workload: uniform unit cube, log-normal masses summing to 1."""
+    mass, pos = np.empty(n), np.empty((n, 3))
+    lib().orc_gen_uniform_lognormal(n, sigma, seed, _ptr(mass, _dp), _ptr(pos, _dp))
+    return mass, pos
+
+
+def gen_clusters(n, nclust=64, amin=1e-3, amax=1e-1, seed=3, velocities=True):
+    """Benchmark workload: nclust Plummer spheres, Dirichlet(1) sizes."""
+    mass, pos = np.empty(n), np.empty((n, 3))
+    vel = np.empty((n, 3)) if velocities else None
+    lib().orc_gen_clusters(n, nclust, amin, amax, seed, _ptr(mass, _dp), _ptr(pos, _dp), _ptr(vel, _dp))
+    return mass, pos, vel
 
 
 def rng_units(seed: int, n: int):
@@ -273,6 +301,13 @@ class Fmm:
         lib().orc_fmm_run(self._h, self.n, _ptr(pos, _dp), _ptr(mass, _dp), nthreads, _ptr(acc, _dp),
                           _ptr(pot, _dp))
         return acc, pot
+
+    def walk(self, nthreads=1):
+        """Moments, power, f pre-pass and the dual walk's record phase only
+        (the walk statistics of crates/bench/src/main.rs:554-641); returns
+        (mutual M2L pairs, P2P leaf pairs incl. self pairs, pops)."""
+        lib().orc_fmm_walk(self._h, self.n, _ptr(self.pos, _dp), _ptr(self.mass, _dp), nthreads)
+        return int(lib().orc_fmm_n_m2l(self._h)), int(lib().orc_fmm_n_p2p(self._h)), self.pops
 
     @property
     def ncells(self):

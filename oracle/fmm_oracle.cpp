@@ -13,14 +13,16 @@
 // Citations are file:line inside crates/fmm/src unless stated otherwise.
 //
 // Parity pinning: the reference is Rust and no Rust toolchain is available, so
-// the reference cannot be run to produce golden outputs. The restatement is
-// pinned against every known-answer test the reference's own test suite holds
-// (tests/test_oracle.py), and the fixtures under tests/golden are generated
-// from it by tests/golden/make_golden.py.
+// the reference cannot be run here. The restatement is pinned against every
+// known-answer test the reference's own test suite holds and against the
+// end-to-end outputs the reference publishes (the N = 1e4 exit-gate errors,
+// todo.md:586; the N = 1e6 walk statistics, PERF-ANALYSIS.md:50-52), all in
+// tests/test_oracle.py.
 //
 // Extensions beyond the reference (flagged in every entry point): Plummer
-// softening in P2P and the direct sum, a geometric opening-angle MAC, and a
-// multi-threaded evaluation used only as the timed CPU baseline.
+// softening in P2P and the direct sum, a geometric opening-angle MAC, a
+// multi-threaded evaluation used only as the timed CPU baseline, and the
+// generators of the benchmark workloads (which have no reference counterpart).
 
 #include <algorithm>
 #include <atomic>
@@ -100,6 +102,105 @@ static void hernquist(size_t n, const double c[3], uint64_t seed, double* mass, 
         pos[3 * i + 0] = c[0] + r * sp * std::cos(phi);
         pos[3 * i + 1] = c[1] + r * sp * std::sin(phi);
         pos[3 * i + 2] = c[2] + r * z;
+    }
+}
+
+// ------------------------------------------------------- benchmark workloads
+// No reference counterpart: the seeded inputs of the benchmark configurations,
+// drawn from the SplitMix64 stream above. The engine's generators
+// (fmmx_gen_plummer_ic, fmmx_gen_uniform_lognormal, fmmx_gen_clusters) must
+// give the same bits; the CPU benchmark arm uses these so that it loads
+// nothing but the oracle.
+
+// Box-Muller normal deviate, the form of crates/fmm/tests/energy_gate.rs:31-35.
+static double normal_dev(Rng& rng) {
+    double u1 = rng.unit();
+    if (u1 < 1e-15) u1 = 1e-15;
+    double u2 = rng.unit();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+}
+
+// Plummer sphere, mass mtot, scale radius a, centre c: the radius by the
+// inverse CDF of models.rs:40-43, redrawn until r <= rmax (in units of a); an
+// isotropic direction; with vel, a speed q * v_esc(r) with q drawn by
+// rejection from q^2 (1 - q^2)^(7/2) (the Plummer distribution function;
+// Aarseth, Henon & Wielen 1974) and an isotropic velocity direction.
+static void workload_plummer(Rng& rng, size_t n, double mtot, double a, double rmax, const double c[3],
+                             double* mass, double* pos, double* vel) {
+    const double mi = mtot / (double)n;
+    for (size_t i = 0; i < n; ++i) {
+        double r;
+        for (;;) {
+            double w = std::pow(rng.unit(), 2.0 / 3.0);
+            r = std::sqrt(w / (1.0 - w));
+            if (r <= rmax) break;
+        }
+        double ct = 2.0 * rng.unit() - 1.0;
+        double ph = 2.0 * M_PI * rng.unit();
+        double st = std::sqrt(1.0 - ct * ct);
+        mass[i] = mi;
+        pos[3 * i + 0] = c[0] + a * r * st * std::cos(ph);
+        pos[3 * i + 1] = c[1] + a * r * st * std::sin(ph);
+        pos[3 * i + 2] = c[2] + a * r * ct;
+        if (!vel) continue;
+        double q;
+        for (;;) {
+            q = rng.unit();
+            double y = 0.1 * rng.unit();
+            if (!(y > q * q * std::pow(1.0 - q * q, 3.5))) break;
+        }
+        double speed = q * std::sqrt(2.0 * mtot / (a * std::sqrt(1.0 + r * r)));
+        double vc = 2.0 * rng.unit() - 1.0;
+        double vp = 2.0 * M_PI * rng.unit();
+        double vs = std::sqrt(1.0 - vc * vc);
+        vel[3 * i + 0] = speed * vs * std::cos(vp);
+        vel[3 * i + 1] = speed * vs * std::sin(vp);
+        vel[3 * i + 2] = speed * vc;
+    }
+}
+
+// Uniform positions in [0,1)^3 and masses exp(sigma N(0,1)), normalised to 1.
+static void workload_uniform(size_t n, double sigma, uint64_t seed, double* mass, double* pos) {
+    Rng rng(seed);
+    double sum = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) pos[3 * i + d] = rng.unit();
+        mass[i] = std::exp(sigma * normal_dev(rng));
+        sum += mass[i];
+    }
+    for (size_t i = 0; i < n; ++i) mass[i] /= sum;
+}
+
+// k Plummer spheres (truncated at 20 a): per sphere an Exp(1) weight, a scale
+// radius log-uniform in [amin, amax] and a centre uniform in [0,1)^3; sizes
+// floor(n w_k / sum w) with the remainder handed out one by one from sphere 0;
+// every body of mass 1/n.
+static void workload_clusters(size_t n, int k, double amin, double amax, uint64_t seed, double* mass, double* pos,
+                              double* vel) {
+    Rng rng(seed);
+    std::vector<double> w(k), a(k), c(3 * (size_t)k);
+    double wsum = 0.0;
+    for (int j = 0; j < k; ++j) {
+        w[j] = -std::log(1.0 - rng.unit());
+        wsum += w[j];
+        a[j] = amin * std::exp(std::log(amax / amin) * rng.unit());
+        c[3 * j] = rng.unit();
+        c[3 * j + 1] = rng.unit();
+        c[3 * j + 2] = rng.unit();
+    }
+    std::vector<size_t> cnt(k);
+    size_t total = 0;
+    for (int j = 0; j < k; ++j) {
+        cnt[j] = (size_t)std::floor((double)n * w[j] / wsum);
+        total += cnt[j];
+    }
+    for (size_t j = 0; total < n; ++j, ++total) cnt[j % k] += 1;
+    size_t at = 0;
+    for (int j = 0; j < k; ++j) {
+        if (!cnt[j]) continue;
+        workload_plummer(rng, cnt[j], (double)cnt[j] * (1.0 / (double)n), a[j], 20.0, &c[3 * j], mass + at,
+                         pos + 3 * at, vel ? vel + 3 * at : nullptr);
+        at += cnt[j];
     }
 }
 
@@ -1199,7 +1300,11 @@ struct Fmm {
 // threads parallelise the independent phases (bit-identical moments, f pre-pass,
 // L2L and L2P; walk replay in parallel with per-thread accumulators reduced in
 // thread order, as walk.rs:490-622 does).
-static void run(Fmm& F, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot) {
+// lists_only: stop after the walk has recorded the interaction lists (the
+// walk statistics of the reference's profile mode, crates/bench/src/main.rs:
+// 554-641, without the translations).
+static void run(Fmm& F, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot,
+                bool lists_only = false) {
     const Tree& t = F.tree;
     size_t p = F.p, d = dimp(p), nc = t.cells.size();
     F.n = n;
@@ -1252,6 +1357,10 @@ static void run(Fmm& F, size_t n, const double* pos, const double* mass, int nth
     F.mc.fmin = F.fmin.data();
     std::vector<Cx> locals(nc * d, CZERO);
     F.lists = WalkOut();
+    if (lists_only) {
+        dual_walk(b, t, F.mc, F.moments.data(), locals.data(), nullptr, false, F.soft2, F.lists);
+        return;
+    }
     if (nthreads <= 1) {
         RotCtx* rot = nullptr;
         RotCtx rc(p >= ROT_P ? p : 0);
@@ -1382,6 +1491,19 @@ void orc_hernquist(size_t n, double cx0, double cy0, double cz0, uint64_t seed, 
     double c[3] = {cx0, cy0, cz0};
     hernquist(n, c, seed, mass, pos);
 }
+void orc_gen_plummer_ic(size_t n, double mtot, double a, double rmax, uint64_t seed, double* mass, double* pos,
+                        double* vel) {
+    Rng rng(seed);
+    const double c[3] = {0.0, 0.0, 0.0};
+    workload_plummer(rng, n, mtot, a, rmax, c, mass, pos, vel);
+}
+void orc_gen_uniform_lognormal(size_t n, double sigma, uint64_t seed, double* mass, double* pos) {
+    workload_uniform(n, sigma, seed, mass, pos);
+}
+void orc_gen_clusters(size_t n, int k, double amin, double amax, uint64_t seed, double* mass, double* pos,
+                      double* vel) {
+    workload_clusters(n, k, amin, amax, seed, mass, pos, vel);
+}
 void orc_rng_units(uint64_t seed, size_t n, double* out) {
     Rng r(seed);
     for (size_t i = 0; i < n; ++i) out[i] = r.unit();
@@ -1427,6 +1549,11 @@ void orc_fmm_free(void* h) { delete (Fmm*)h; }
 void orc_fmm_set_gap(void* h, double gap) { ((Fmm*)h)->gap = gap; }
 void orc_fmm_run(void* h, size_t n, const double* pos, const double* mass, int nthreads, double* acc, double* pot) {
     run(*(Fmm*)h, n, pos, mass, nthreads, acc, pot);
+}
+// Moments, power, f pre-pass and the walk's record phase only: the lists and
+// counters of an evaluation without its translations.
+void orc_fmm_walk(void* h, size_t n, const double* pos, const double* mass, int nthreads) {
+    run(*(Fmm*)h, n, pos, mass, nthreads, nullptr, nullptr, true);
 }
 size_t orc_fmm_ncells(void* h) { return ((Fmm*)h)->tree.cells.size(); }
 // Cell export: first, count, level, leaf (u32 x4 per cell), children (i32 x8),

@@ -74,3 +74,13 @@ def test_generator_matches_reference_sampler(orc):
     m1, p1 = fx.gen_hernquist(3000, center=(1.0, -2.0, 0.5), seed=7)
     m2, p2 = orc.hernquist(3000, center=(1.0, -2.0, 0.5), seed=7)
     assert np.array_equal(p1, p2)
+
+
+def test_noalloc_limit_matches_header():
+    """The Python constant of the allocation-free direct sum's target limit is
+    the header's FMMX_DIRECT_NOALLOC_MAX_TARGETS."""
+    import fmms_b200 as fx
+
+    txt = open(os.path.join(ROOT, "include", "fmmx.h")).read()
+    m = re.search(r"#define\s+FMMX_DIRECT_NOALLOC_MAX_TARGETS\s+(\d+)", txt)
+    assert m and int(m.group(1)) == fx.DIRECT_NOALLOC_MAX_TARGETS

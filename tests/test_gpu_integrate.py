@@ -127,3 +127,100 @@ def test_graph_replay_matches_launches(precision):
             out.append(run_leapfrog(mass, pos, vel, kw, 1e-3, 11, "kdk", 4))
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_graph_dropped_by_new_lists(precision):
+    """A full evaluation between two graph-replayed leapfrog calls rebuilds the
+    interaction lists (new buffers and sizes); the next leapfrog call must not
+    replay the graph recorded against the old lists. Bitwise equal to the same
+    sequence without graphs."""
+    import torch
+
+    import fmms_b200 as fx
+
+    mass, pos, vel = fx.gen_plummer_ic(8192, seed=21)
+    n = len(mass)
+    side = torch.cuda.Stream()
+    out = []
+    counts = []
+    for graphs in (False, True):
+        # the reference MAC: its decisions follow the moments, so the walk on
+        # moved bodies gives other lists for the same tree
+        kw = dict(p=8, eps=1e-5, n_leaf=32, softening=1e-3, precision=precision, use_graphs=graphs)
+        with torch.cuda.stream(side):
+            d_pos = torch.from_numpy(pos.copy()).cuda()
+            d_vel = torch.from_numpy(vel.copy()).cuda()
+            d_mass = torch.from_numpy(mass).cuda()
+            d_acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+            d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+            g = fx.Fmm(None, None, **kw, stream=side.cuda_stream)
+            ptrs = (d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+            g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+            g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+            g.leapfrog_device(*ptrs, 1e-3, 3, "kdk", 8)  # records and replays a graph
+            c0 = (g.stats()["n_m2l"], g.stats()["n_p2p"])
+            # move the bodies so that the walk changes, then a full evaluation
+            d_pos.mul_(1.3)
+            g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+            counts.append((c0, (g.stats()["n_m2l"], g.stats()["n_p2p"])))
+            g.leapfrog_device(*ptrs, 1e-3, 3, "kdk", 8)
+            side.synchronize()
+            out.append([t.cpu().numpy() for t in (d_pos, d_vel, d_acc, d_pot)])
+            g.close()
+    assert counts[0][0] != counts[0][1]  # the lists did change
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+def test_energy_gate_mixed(orc):
+    """Mixed form on the reference's energy-gate setup (energy_gate.rs:143-219
+    with the smoke's IC, :235-251): a virialised Plummer sphere, here N = 2^16
+    with the reference MAC (eps 1e-5, p 8, leaf 16), 400 kick-drift-kick steps
+    of dt = 1e-3 with a rebuild every step. The gate of :253-290 on energy:
+    drift and maximum deviation < 1e-3, secular slope < 1e-6 per step; the
+    drift is also checked in each window of 100 steps. Momentum: the mixed
+    form's near field is FP32, so its bound is 1e-6 instead of 1e-12."""
+    import torch
+
+    import fmms_b200 as fx
+
+    n, steps, dt = 1 << 16, 400, 1e-3
+    mass, pos = fx.gen_plummer(n, seed=42)
+    kw = dict(p=8, eps=1e-5, n_leaf=16, precision="mixed")
+    pot0 = fx.Fmm(mass, pos, **kw).run().pot
+    vel = warm_start(orc, mass, pos, pot0)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        d_pos = torch.from_numpy(pos.copy()).cuda()
+        d_vel = torch.from_numpy(vel.copy()).cuda()
+        d_mass = torch.from_numpy(mass).cuda()
+        d_acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+        g = fx.Fmm(None, None, **kw, stream=side.cuda_stream)
+        g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+        g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+
+        def e_now():
+            return float((0.5 * (d_mass * (d_vel * d_vel).sum(1)).sum() - 0.5 * (d_mass * d_pot).sum()).item())
+
+        e0 = e_now()
+        es = []
+        for _ in range(steps):
+            g.leapfrog_device(d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
+                              d_pot.data_ptr(), dt, 1, "kdk", 1)
+            es.append(e_now())
+        v = d_vel.cpu().numpy()
+        g.close()
+    es = np.array(es)
+    assert abs(e0 + 0.147) < 0.03
+    drift = (es[-1] - e0) / abs(e0)
+    max_dev = np.max(np.abs(es - e0)) / abs(e0)
+    t = np.arange(1, steps + 1, dtype=float)
+    slope = np.polyfit(t, es, 1)[0] / abs(e0)
+    windows = [(es[k + 99] - (es[k - 1] if k else e0)) / abs(e0) for k in range(0, steps, 100)]
+    assert abs(drift) < 1e-3, drift
+    assert max_dev < 1e-3, max_dev
+    assert abs(slope) < 1e-6, slope
+    assert max(abs(w) for w in windows) < 1e-3, windows
+    assert momentum_rel(mass, v) < 1e-6

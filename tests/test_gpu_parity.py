@@ -233,3 +233,54 @@ def test_full_size_c2_plain(orc):
     rp = rel_rows(res.pot, pot_o)
     assert ra.max() < ACC_TOL, f"acc rel err {ra.max():.3e}"
     assert rp.max() < ACC_TOL, f"pot rel err {rp.max():.3e}"
+
+
+def test_c1_plummer_ic(orc):
+    """The C1 workload through its own generator (Plummer sphere truncated at
+    r <= 20, distribution-function velocities; N = 16384, softening 1e-3, p 8,
+    theta 0.5, leaf 64) on the full parity bar."""
+    mass, pos, _ = fx().gen_plummer_ic(16384, 1.0, 1.0, 20.0, 11)
+    check_case(orc, mass, pos, 8, 0.0, 64, mac="theta", theta=0.5, softening=1e-3)
+
+
+@pytest.mark.parametrize("p", [4, 8])
+def test_naive_m2l(orc, p):
+    """m2l='naive' (k_m2l_naive_f64, the reference's O(p^4) convolution of
+    translate.rs:47-136) against the oracle: same lists, locals and forces."""
+    mass, pos = orc.plummer(8192, seed=17)
+    check_case(orc, mass, pos, p, 1e-5, 16, m2l="naive")
+    mass, pos, _ = fx().gen_plummer_ic(8192, 1.0, 1.0, 20.0, 3)
+    check_case(orc, mass, pos, p, 0.0, 32, m2l="naive", mac="theta", theta=0.5, softening=1e-3)
+
+
+def test_c3_clusters_plain(orc):
+    """The clustered deep-tree workload's generator and settings (64 Plummer
+    clusters, scale radii log-uniform in [1e-3, 1e-1], leaf 32, p 12, theta
+    0.4, softening 1e-5) at N = 2^20 on the plain form: Morton keys, slot
+    order, every cell field, both pair sets equal to the oracle's, and
+    accelerations and potentials within 1e-12 relative per body (oracle
+    threaded on the host)."""
+    import os
+
+    mass, pos, _ = fx().gen_clusters(1 << 20, 64, 1e-3, 1e-1, 33)
+    kw = dict(mac="theta", theta=0.4, softening=1e-5)
+    g = fx().Fmm(mass, pos, 12, 0.0, 32, **kw)
+    res = g.run()
+    o = orc.Fmm(mass, pos, 12, 0.0, 32, mac=orc.MAC_THETA, theta=0.4, softening=1e-5)
+    acc_o, pot_o = o.run(nthreads=os.cpu_count() or 1)
+    order_g, keys_g, cells_g = g.export_tree()
+    order_o, keys_o = o.order()
+    assert np.array_equal(keys_g, keys_o)
+    assert np.array_equal(order_g, order_o)
+    cells_o = o.cells()
+    for k in ("first", "count", "level", "leaf", "children", "cen", "mass", "rho"):
+        assert np.array_equal(cells_g[k], cells_o[k]), k
+    assert cells_g["level"].max() >= 12  # a deep tree
+    m2l_g, p2p_g = g.export_lists()
+    m2l_o, p2p_o = o.lists()
+    assert np.array_equal(pair_set(m2l_g), pair_set(m2l_o))
+    assert np.array_equal(pair_set(p2p_g), pair_set(p2p_o))
+    ra = rel_rows(res.accel, acc_o)
+    rp = rel_rows(res.pot, pot_o)
+    assert ra.max() < ACC_TOL, f"acc rel err {ra.max():.3e}"
+    assert rp.max() < ACC_TOL, f"pot rel err {rp.max():.3e}"

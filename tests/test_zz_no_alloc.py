@@ -56,6 +56,37 @@ def test_noalloc_direct_matches_allocating_form_on_two_calls():
         assert np.max(_rel(d_f.cpu().numpy(), f_ref)) < TOL
 
 
+def test_noalloc_out_of_range_target_is_nan_only_there():
+    """A target id >= n cannot be checked on the host (the ids are in device
+    memory): that target's results are NaN, every other target's are exact."""
+    import torch
+
+    import fmms_b200 as fx
+
+    stream = torch.cuda.current_stream()
+    n, nt = 5000, 64
+    mass, pos = fx.gen_plummer(n, seed=31)
+    t = np.arange(0, 2 * nt, 2, dtype=np.uint32)
+    a_ref, p_ref, f_ref = fx.direct_targets(mass, pos, t, softening=1e-3)
+    bad = t.copy()
+    bad[5] = n + 7
+    d_pos = torch.from_numpy(pos).cuda()
+    d_mass = torch.from_numpy(mass).cuda()
+    d_t = torch.from_numpy(bad.view(np.int32)).cuda()
+    d_acc = torch.zeros((nt, 3), dtype=torch.float64, device="cuda")
+    d_pot = torch.zeros((nt,), dtype=torch.float64, device="cuda")
+    d_f = torch.zeros((nt,), dtype=torch.float64, device="cuda")
+    fx.direct_targets_noalloc(n, d_pos.data_ptr(), d_mass.data_ptr(), nt, d_t.data_ptr(), d_acc.data_ptr(),
+                              d_pot.data_ptr(), d_f.data_ptr(), softening=1e-3, device=0, stream=stream.cuda_stream)
+    stream.synchronize()
+    acc, pot, f = d_acc.cpu().numpy(), d_pot.cpu().numpy(), d_f.cpu().numpy()
+    ok = np.arange(nt) != 5
+    assert np.all(np.isnan(acc[5])) and np.isnan(pot[5]) and np.isnan(f[5])
+    assert np.max(_rel(acc[ok], a_ref[ok])) < TOL
+    assert np.max(_rel(pot[ok], p_ref[ok])) < TOL
+    assert np.max(_rel(f[ok], f_ref[ok])) < TOL
+
+
 def test_noalloc_rejects_more_targets_than_its_scratch_holds():
     import fmms_b200 as fx
 
