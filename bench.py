@@ -1,16 +1,25 @@
 #!/usr/bin/env python
-"""Benchmark of the FMM force evaluation on B200.
+"""Benchmark of the FMM force engine on B200.
 
-Metric: bodies/s of one complete force evaluation (tree build, upward pass,
-dual walk, M2L, L2L, P2P, L2P) on one GPU, with the p50/p99 relative force
-error against an FP64 direct sum on 4096 seeded targets beside it.
+Metric: bodies/s of kick-drift-kick leapfrog steps (each a complete force
+evaluation: tree build, upward pass, dual walk, lists, M2L, L2L, P2P, L2P)
+on one GPU, in the mixed-precision form against the plain FP64 form, both at
+a setting where the p99 relative force error against the FP64 direct sum on
+4096 seeded targets is <= 1e-5; p50/p99 step times beside it.
 
-Workload (default, --config c2): N = 1,048,576 bodies uniform in the unit cube,
-log-normal masses (mu 0, sigma 0.5) normalised to 1, Plummer softening 1e-4,
-p = 10, opening angle 0.5, leaf capacity 64; seeded synthetic data.
+Workload (default, --config c3): the clustered deep-tree system, N = 4,194,304
+bodies in 64 Plummer spheres (scale radii log-uniform in [1e-3, 1e-1], centres
+uniform in the unit cube, Dirichlet(1) sizes, equal masses summing to 1,
+distribution-function velocities), softening 1e-5, leaf capacity 32, KDK steps
+of dt = 1e-4 with a rebuild every step; seeded synthetic data. The configured
+order and opening angle (p = 12, theta = 0.4) leave p99 at 2.1e-4 in both
+forms (the unsoftened far field against a softened direct sum); the bench runs
+p = 10, theta = 0.5 with M2L pairs kept soft_gap = 200 softening lengths
+apart, where both forms meet the bound.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|plain]
-    python bench.py --impl reference ...   # CPU FMM (the oracle's restatement)
+    python bench.py --config c2 ...         # one force evaluation, N = 2^20 uniform cube
+    python bench.py --impl reference ...    # the reference FMM on the host cores (oracle/)
 
 Under torchrun every rank runs its own replica (the evaluation does not shard;
 no collective on the data path); rank 0 prints one JSON line.
@@ -40,6 +49,13 @@ CONFIGS = {
     "c3": dict(gen="clusters", n=1 << 22, p=12, theta=0.4, softening=1e-5, n_leaf=32,
                workload="64 Plummer clusters N=4194304, a log-uniform[1e-3,1e-1], softening 1e-5, p=12, theta=0.4, leaf 32"),
 }
+# The headline: the clustered system in KDK steps at the setting where both
+# forms meet p99 <= 1e-5 (from the accuracy sweep, --config c3 --sweep).
+HEADLINE = dict(CONFIGS["c3"], p=10, theta=0.5, soft_gap=200.0, dt=1e-4,
+                workload="64 Plummer clusters N=4194304 (a log-uniform[1e-3,1e-1], Dirichlet(1) sizes, DF velocities), "
+                         "softening 1e-5, leaf 32, KDK steps dt=1e-4 with a rebuild every step; p=10, theta=0.5, "
+                         "soft_gap=200 (both forms meet p99<=1e-5 there; the configured p=12, theta=0.4 give "
+                         "p99 2.1e-4 in both forms)")
 EXTRA_CONFIGS = {
     "c4": dict(gen="ensemble", n=0, p=8, theta=0.5, softening=1e-3, n_leaf=64, workload="ensemble"),
     "c5": dict(gen="serve", n=0, p=8, theta=0.5, softening=1e-3, n_leaf=64, workload="serving"),
@@ -48,15 +64,19 @@ SEEDS = {"plummer_ic": 11, "uniform": 22, "clusters": 33}
 METRIC = "bodies/s at p99 force err <=1e-5 (mixed vs FP64 plain, 1 B200); p50/p99 step ms"
 
 
-def make_inputs(fx, cfg):
+def make_inputs(gen, cfg, velocities=False):
+    """Seeded inputs of a configuration from `gen`: the engine package
+    (fmms_b200) in the GPU arm, the oracle in the CPU arm (the two give the
+    same bits, tests/test_generators.py)."""
     n = cfg["n"]
     if cfg["gen"] == "uniform":
-        mass, pos = fx.gen_uniform_lognormal(n, 0.5, SEEDS["uniform"])
+        mass, pos = gen.gen_uniform_lognormal(n, 0.5, SEEDS["uniform"])
+        vel = np.zeros_like(pos)
     elif cfg["gen"] == "plummer_ic":
-        mass, pos, _ = fx.gen_plummer_ic(n, 1.0, 1.0, 20.0, SEEDS["plummer_ic"])
+        mass, pos, vel = gen.gen_plummer_ic(n, 1.0, 1.0, 20.0, SEEDS["plummer_ic"])
     else:
-        mass, pos, _ = fx.gen_clusters(n, 64, 1e-3, 1e-1, SEEDS["clusters"])
-    return mass, pos
+        mass, pos, vel = gen.gen_clusters(n, 64, 1e-3, 1e-1, SEEDS["clusters"])
+    return (mass, pos, vel) if velocities else (mass, pos)
 
 
 # ------------------------------------------------------------------ roofline
@@ -148,49 +168,100 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU arm
-def cpu_fmm_sample(cfg, sample_n, nthreads, fx):
-    """Time the oracle's restatement of the reference FMM (threaded run_impl)
-    on a bounded sample of the workload; returns (bodies/s, seconds)."""
+def oracle_fmm(cfg, mass, pos):
+    import oracle
+
+    return oracle.Fmm(mass, pos, cfg["p"], 0.0, cfg["n_leaf"], mac=oracle.MAC_THETA, theta=cfg["theta"],
+                      softening=cfg["softening"], soft_gap=cfg.get("soft_gap", 0.0))
+
+
+def cpu_fmm_sample(cfg, sample_n, nthreads):
+    """Time the oracle's restatement of the reference FMM (tree build and the
+    threaded run_impl) on a bounded sample of the workload (the same generator
+    at sample_n bodies); returns (bodies/s, seconds)."""
     import oracle
 
     sub = dict(cfg)
     sub["n"] = sample_n
-    mass, pos = make_inputs(fx, sub)
+    mass, pos = make_inputs(oracle, sub)
     t0 = time.perf_counter()
-    f = oracle.Fmm(mass, pos, cfg["p"], 0.0, cfg["n_leaf"], mac=oracle.MAC_THETA, theta=cfg["theta"],
-                   softening=cfg["softening"])
+    f = oracle_fmm(cfg, mass, pos)
     f.run(nthreads=nthreads)
     dt = time.perf_counter() - t0
     return sample_n / dt, dt
 
 
-def run_reference(args, cfg, rank):
-    """--impl reference: the reference's CPU FMM (restated in oracle/, the
-    Rust reference cannot be built here) on the box's host cores."""
+def run_reference(args, cfg, rank, headline):
+    """--impl reference: the reference FMM on the box's host cores, restated in
+    oracle/ (the Rust reference cannot be built here: no Rust toolchain). It
+    loads nothing but the oracle. The headline arm runs the same system at the
+    same N and settings: each step a kick-drift-kick step whose force
+    evaluation is the oracle's tree build (Fmm::refresh) and threaded run
+    (Fmm::run_threaded) on all host threads, the kicks and drifts on the host;
+    the warm-up steps run on a 65,536-body system of the same generator (the
+    CPU arm has nothing to warm but its allocator). --ref-sample N times an
+    N-body sample instead of the full system."""
     if rank != 0:
         return
-    import fmms_b200 as fx
+    import oracle
 
     nthreads = os.cpu_count() or 1
-    sample_n = args.cpu_sample
+    full = cfg["n"]
+    sample_n = args.ref_sample if args.ref_sample > 0 else full
+    sub = dict(cfg, n=sample_n)
+    mass, pos, vel = make_inputs(oracle, sub, velocities=True)
+    warm = dict(cfg, n=min(65536, sample_n))
+    wm, wp = make_inputs(oracle, warm)
+    for _ in range(args.warmup):
+        oracle_fmm(cfg, wm, wp).run(nthreads=nthreads)
+    dt_step = cfg.get("dt", 0.0)
+    f = oracle_fmm(cfg, mass, pos)
+    acc, _ = f.run(nthreads=nthreads)
     times = []
-    for i in range(args.warmup + args.steps):
-        bps, dt = cpu_fmm_sample(cfg, sample_n, nthreads, fx)
-        if i >= args.warmup:
-            times.append(dt)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        if headline:  # kick-drift-kick around a rebuild and a threaded evaluation
+            vel += 0.5 * dt_step * acc
+            pos += dt_step * vel
+            f.refresh(mass, pos)
+            acc, _ = f.run(nthreads=nthreads)
+            vel += 0.5 * dt_step * acc
+        else:
+            f.refresh(mass, pos)
+            f.run(nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
     mean = sum(times) / len(times)
     value = sample_n / mean
+    what = ("one kick-drift-kick step (oracle tree build + threaded evaluation, host kicks and drifts)"
+            if headline else "one force evaluation (oracle tree build + threaded evaluation)")
+    sample = (f"the full system ({sample_n} bodies)" if sample_n == full else
+              f"{sample_n} bodies of the same generator and settings")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "sample_bodies": sample_n},
+        "config": bench_config(cfg, args.gpus, headline),
+        "step_ms_p50": float(np.percentile(times, 50)) * 1e3, "step_ms_p99": float(np.percentile(times, 99)) * 1e3,
         "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{sample_n} bodies of the same generator and settings, one threaded "
-                                   f"evaluation per step (oracle/fmm_oracle.cpp run_impl)"},
+                         "sample": f"{sample}, {what} per step, on {nthreads} host threads; warm-up steps on "
+                                   f"{warm['n']} bodies (oracle/fmm_oracle.cpp, the C++ restatement of "
+                                   f"crates/fmm run_impl)"},
         "e2e": {"value": value, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def bench_config(cfg, world, headline):
+    """The `config` object of the JSON line; the same in both arms."""
+    c = {"workload": cfg["workload"], "n": cfg["n"], "p": cfg["p"], "theta": cfg["theta"],
+         "softening": cfg["softening"], "n_leaf": cfg["n_leaf"]}
+    if headline:
+        c.update(soft_gap=cfg["soft_gap"], dt=cfg["dt"], refresh_every=1,
+                 l2="flushed between timed steps (and the inputs are larger than L2)")
+    else:
+        c.update(l2="flushed between timed steps")
+    c["parallelism"] = "replicas" if world > 1 else "single"
+    return c
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -306,8 +377,7 @@ class _NullCtx:
 # DRAM bytes (read + write) per directed M2L translation, from one ncu capture of
 # the M2L launch at N = 262144 (uniform cube, p = 10, theta 0.5, leaf 64: 5,809,554
 # directed translations); the expansions are L2-resident, so the traffic grows
-# with the translation count. See profiles/m2l_rotw_f32_p10_n262144.md and
-# profiles/m2l_rotw_f64_p10_n262144.md.
+# with the translation count.
 M2L_DRAM_BYTES_PER_TRANSLATION = {("mixed", 10): (34.537728e6 + 0.07424e6) / 5809554,
                                   ("plain", 10): (84.023808e6 + 21.590272e6) / 5809554}
 
@@ -315,7 +385,7 @@ M2L_DRAM_BYTES_PER_TRANSLATION = {("mixed", 10): (34.537728e6 + 0.07424e6) / 580
 def roofline(args, cfg, r, precision, dev):
     import fmms_b200 as fx
 
-    st = r["st"]
+    st = r.get("solo_st") or r["st"]  # the counts of the evaluations the kernels were timed in
     kernel = "naive" if args.m2l == "naive" else "rotation"
     fl = st["m2l_directed"] * m2l_flops_per_translation(cfg["p"], kernel)
     fp64 = precision == "plain"
@@ -360,7 +430,7 @@ def run_gpu(args, cfg, rank, world, local_rank):
     cpu = None
     if world == 1 and not args.no_cpu:
         nth = os.cpu_count() or 1
-        bps, dt = cpu_fmm_sample(cfg, args.cpu_sample, nth, fx)
+        bps, dt = cpu_fmm_sample(cfg, args.cpu_sample, nth)
         cpu = {"value": bps, "unit": "bodies/s", "cores": nth, "kind": "port",
                "sample": f"{args.cpu_sample} bodies of the same generator and settings, one threaded evaluation "
                          f"of the oracle's restatement of the reference FMM ({dt:.1f} s)"}
@@ -369,9 +439,7 @@ def run_gpu(args, cfg, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": main["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "precision": args.precision, "n": n, "p": cfg["p"],
-                   "theta": cfg["theta"], "n_leaf": cfg["n_leaf"], "l2": "flushed between timed steps",
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "precision": args.precision, "config": bench_config(cfg, world, False),
         "step_ms_p50": float(np.percentile(main["times"], 50)),
         "step_ms_p99": float(np.percentile(main["times"], 99)),
         "force_err": {"p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99)),
@@ -390,6 +458,188 @@ def run_gpu(args, cfg, rank, world, local_rank):
                            "ms_per_step": other["total_ms"] / args.steps,
                            "force_err_p50": float(np.percentile(orel, 50)),
                            "force_err_p99": float(np.percentile(orel, 99)),
+                           "stages_ms": {k[3:]: round(v, 3) for k, v in other["st"].items() if k.startswith("ms_")},
+                           "speedup_of_main": value / ov}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ headline: C3 KDK steps
+def measure_kdk(args, cfg, precision, mass, pos, vel, tg, dev, world, clk_sampler=None):
+    """W untimed and K timed kick-drift-kick steps (a rebuild every step) on
+    device-resident state, the force error against the FP64 direct sum at the
+    seeded targets after every timed step; then the same steps end to end
+    through the host API (pinned host buffers, the reference's loop:
+    host kick and drift, Fmm::refresh = fmmx_build, Fmm::run = fmmx_evaluate);
+    then the M2L and P2P alone on the device for the roofline."""
+    import torch
+
+    import fmms_b200 as fx
+
+    stream = torch.cuda.current_stream()
+    n = len(mass)
+    cuda = f"cuda:{dev}"
+    d_pos = torch.from_numpy(pos.copy()).to(cuda)
+    d_vel = torch.from_numpy(vel.copy()).to(cuda)
+    d_mass = torch.from_numpy(mass).to(cuda)
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=cuda)
+    d_pot = torch.empty(n, dtype=torch.float64, device=cuda)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=cuda)
+    d_tg = torch.from_numpy(tg.view(np.int32)).to(cuda)
+    t_idx = torch.from_numpy(tg.astype(np.int64)).to(cuda)
+    d_aref = torch.empty((len(tg), 3), dtype=torch.float64, device=cuda)
+    kw = dict(mac="theta", theta=cfg["theta"], softening=cfg["softening"], precision=precision, m2l=args.m2l,
+              soft_gap=cfg["soft_gap"], device=dev, stream=stream.cuda_stream)
+    g = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], **kw)
+    ptrs = (d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+    g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+    g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+
+    def step():
+        g.leapfrog_device(*ptrs, cfg["dt"], 1, "kdk", 1)
+
+    def force_err():  # the FP64 direct sum at the targets, on the device (no allocation)
+        fx.direct_targets_noalloc(n, d_pos.data_ptr(), d_mass.data_ptr(), len(tg), d_tg.data_ptr(),
+                                  d_aref.data_ptr(), softening=cfg["softening"], device=dev,
+                                  stream=stream.cuda_stream)
+        rel = torch.linalg.norm(d_acc[t_idx] - d_aref, dim=1) / torch.linalg.norm(d_aref, dim=1)
+        return rel.cpu().numpy()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    times, errs, st = [], [], None
+    with (clk_sampler if clk_sampler is not None else _NullCtx()):
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (untimed)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            st = g.stats()
+            errs.append(force_err())
+    torch.cuda.synchronize()
+    total_ms = sum(times)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], dtype=torch.float64, device=cuda)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        total_ms = float(t.item())
+    g.close()
+
+    # end to end: the reference's loop through the host API
+    h_pos = torch.from_numpy(pos.copy()).pin_memory()
+    h_vel = torch.from_numpy(vel.copy()).pin_memory()
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_acc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    h_pot = torch.empty(n, dtype=torch.float64).pin_memory()
+    xp, xv, xm, xa, xpot = (t.numpy() for t in (h_pos, h_vel, h_mass, h_acc, h_pot))
+    ge = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], **kw)
+    L = fx.lib()
+
+    def host_eval():
+        stb = L.fmmx_build(ge._h, n, fx._ptr(xp), fx._ptr(xm))
+        ste = L.fmmx_evaluate(ge._h, None, None, fx._ptr(xa), fx._ptr(xpot))
+        assert stb == 0 and ste == 0, L.fmmx_last_error(ge._h)
+
+    host_eval()
+    dt = cfg["dt"]
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xv += (0.5 * dt) * xa
+        xp += dt * xv
+        host_eval()
+        xv += (0.5 * dt) * xa
+        if i >= args.warmup:
+            e2e_times.append((time.perf_counter() - t0) * 1e3)
+    ge.close()
+
+    # the M2L and P2P kernels alone on the device (one stream, nothing beside
+    # them), for the roofline; in the timed steps the P2P runs beside the M2L
+    solo = fx.Fmm(None, None, cfg["p"], 0.0, cfg["n_leaf"], **kw, overlap=False)
+    m2l_solo, p2p_solo = [], []
+    for i in range(2 + max(min(args.steps, 5), 1)):
+        flush.zero_()
+        solo.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+        solo.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+        if i >= 2:
+            sst = solo.stats()
+            m2l_solo.append(sst["ms_m2l"])
+            p2p_solo.append(sst["ms_p2p"])
+    solo.close()
+    p99s = [float(np.percentile(e, 99)) for e in errs]
+    p50s = [float(np.percentile(e, 50)) for e in errs]
+    return dict(times=times, total_ms=total_ms, st=st, e2e_ms=float(np.mean(e2e_times)), p99s=p99s, p50s=p50s,
+                m2l_ms=float(np.mean(m2l_solo)), p2p_ms=float(np.mean(p2p_solo)), m2l_ms_in_step=st["ms_m2l"],
+                ntargets=len(tg), solo_st=sst)
+
+
+def run_headline(args, cfg, rank, world, local_rank):
+    import torch
+
+    import fmms_b200 as fx
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    mass, pos, vel = make_inputs(fx, cfg, velocities=True)
+    n = len(mass)
+    tg = np.sort(np.random.default_rng(4096).choice(n, size=min(4096, n), replace=False)).astype(np.uint32)
+    clk = ClockSampler(dev)
+    main = measure_kdk(args, cfg, args.precision, mass, pos, vel, tg, dev, world, clk)
+    other = None
+    if not args.no_compare:
+        other_prec = "plain" if args.precision == "mixed" else "mixed"
+        other = measure_kdk(args, cfg, other_prec, mass, pos, vel, tg, dev, world)
+    if rank != 0:
+        return
+    value = world * n * args.steps / (main["total_ms"] * 1e-3)
+    st = main["st"]
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nth = os.cpu_count() or 1
+        bps, dt = cpu_fmm_sample(cfg, args.cpu_sample, nth)
+        cpu = {"value": bps, "unit": "bodies/s", "cores": nth, "kind": "port",
+               "sample": f"{args.cpu_sample} bodies of the same generator and settings, one tree build and "
+                         f"threaded evaluation of the oracle's restatement of the reference FMM ({dt:.1f} s)"}
+    fp64 = args.precision == "plain"
+    line = {
+        "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": main["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
+        "precision": args.precision, "config": bench_config(cfg, world, True),
+        "step_ms_p50": float(np.percentile(main["times"], 50)),
+        "step_ms_p99": float(np.percentile(main["times"], 99)),
+        "force_err": {"p50": float(np.median(main["p50s"])), "p99": float(np.max(main["p99s"])),
+                      "p99_per_step": main["p99s"], "targets": main["ntargets"],
+                      "reference": "FP64 direct sum, after every timed step; p99 is the largest per-step p99"},
+        "e2e": {"value": world * n / (main["e2e_ms"] * 1e-3), "unit": "bodies/s", "h2d_bytes_per_step": 32 * n,
+                "d2h_bytes_per_step": 32 * n, "ms_per_step": main["e2e_ms"],
+                "path": "host loop as the reference's energy gate: kick and drift on the host, fmmx_build "
+                        "(Fmm::refresh) and fmmx_evaluate (Fmm::run) from pinned host buffers"},
+        "gpu_launches": (int(st["kernel_launches"]) + 3) * args.steps,
+        "stages_ms": {k[3:]: round(v, 3) for k, v in st.items() if k.startswith("ms_")},
+        "counts": {k: int(st[k]) for k in ("n_cells", "n_leaves", "n_m2l", "n_p2p", "p2p_interactions")},
+        "roofline": roofline(args, cfg, main, args.precision, dev), "cpu_baseline": cpu, "clocks": clk.summary(),
+    }
+    if other is not None:
+        ov = world * n * args.steps / (other["total_ms"] * 1e-3)
+        line["compare"] = {"precision": "plain" if args.precision == "mixed" else "mixed", "value": ov,
+                           "ms_per_step": other["total_ms"] / args.steps,
+                           "force_err_p50": float(np.median(other["p50s"])),
+                           "force_err_p99": float(np.max(other["p99s"])),
+                           "e2e_value": world * n / (other["e2e_ms"] * 1e-3),
                            "stages_ms": {k[3:]: round(v, 3) for k, v in other["st"].items() if k.startswith("ms_")},
                            "speedup_of_main": value / ov}
     print(json.dumps(line), flush=True)
@@ -746,7 +996,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fmmx", choices=["fmmx", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4", "c5"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS) + ["c4", "c5"])
     ap.add_argument("--precision", default="mixed", choices=["plain", "mixed"])
     ap.add_argument("--no-compare", action="store_true", help="skip the other precision's run")
     ap.add_argument("--kdk-steps", type=int, default=10)
@@ -763,6 +1013,10 @@ def main():
     ap.add_argument("--latency-slo", type=float, default=2.0)
     ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="--impl reference: time an N-body sample instead of the full system (0: full)")
+    ap.add_argument("--kdk", action="store_true",
+                    help="c3: the earlier KDK report at the configured p=12, theta=0.4 (no accuracy bound)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override N (small cases for profiling)")
     ap.add_argument("--graphs", action="store_true",
@@ -770,7 +1024,8 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="c3: force evaluations at several (p, theta) in both precisions, compared at p99 <= 1e-5")
     args = ap.parse_args()
-    cfg = dict(CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config])
+    headline = args.config == "c3" and not (args.sweep or args.kdk or args.graphs)
+    cfg = dict(HEADLINE if headline else (CONFIGS.get(args.config) or EXTRA_CONFIGS[args.config]))
     if args.n > 0:
         cfg["n"] = args.n
         cfg["workload"] += f" (N overridden: {args.n})"
@@ -778,7 +1033,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference(args, cfg, rank)
+        run_reference(args, cfg, rank, headline)
         return
     if world > 1:
         import datetime
@@ -789,8 +1044,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        runner = {"c3": run_accuracy_sweep if args.sweep else run_kdk, "c4": run_ensemble,
-                  "c5": run_serve}.get(args.config, run_gpu)
+        runner = {"c3": run_headline if headline else (run_accuracy_sweep if args.sweep else run_kdk),
+                  "c4": run_ensemble, "c5": run_serve}.get(args.config, run_gpu)
         if args.graphs:
             runner = run_graphs
         runner(args, cfg, rank, world, local_rank)

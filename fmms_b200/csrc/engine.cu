@@ -155,11 +155,13 @@ struct fmmx_ctx {
     uint32_t cap_front = 0, cap_m2l = 0, cap_p2p = 0;
 
     // directed lists
-    DBuf<uint64_t> m2l_keys, m2l_keys_s, p2p_keys, p2p_keys_s;
-    DBuf<uint32_t> m2l_k32, m2l_k32_s, p2p_k32, p2p_k32_s;  // the same when 2 * list_shift <= 32
-    bool keys32 = false;
-    int list_shift = 32;  // keys of the directed lists: (dst << list_shift) | src
-    DBuf<uint32_t> m2l_seg_b, m2l_seg_e, p2p_seg_b, p2p_seg_e;
+    // per destination cell c: sources src[off[c] .. off[c+1]), ascending
+    DBuf<uint32_t> m2l_src_u, m2l_src, p2p_src_u, p2p_src;  // scattered, then sorted within segments
+    DBuf<uint32_t> m2l_off, p2p_off, list_cnt;               // nc + 1 each
+    // near-field work units of the mixed P2P (per leaf: units, scratch bodies)
+    DBuf<uint32_t> p2p_units, p2p_scr, p2p_uoff, p2p_soff;
+    DBuf<double4> p2p_part;
+    DBuf<unsigned> p2p_next;
 
     DBuf<int> work;  // persistent-kernel work counter
     int nsm = 148;
@@ -601,72 +603,48 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
 
 fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
     const int nc = ctx->nc;
-    const int shift = bits_for((uint64_t)nc);  // keys (dst << shift) | src
-    const int cbits = 2 * shift;
-    const bool k32 = cbits <= 32;  // 32-bit keys: half the sort traffic
-    ctx->list_shift = shift;
-    ctx->keys32 = k32;
-    // M2L
-    const int nm = ctx->n_m2l;
-    CK(ctx->m2l_seg_b.ensure(nc), "alloc lists");
-    CK(ctx->m2l_seg_e.ensure(nc), "alloc lists");
-    CK(cudaMemsetAsync(ctx->m2l_seg_b.p, 0, nc * sizeof(uint32_t), s), "memset");
-    CK(cudaMemsetAsync(ctx->m2l_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
-    if (nm > 0) {
-        LCOUNT(3);
-        const unsigned ge = grid_for(nm, 256), gs = grid_for(2 * (size_t)nm, 256);
-        if (k32) {
-            CK(ctx->m2l_k32.ensure(2 * (size_t)nm), "alloc lists");
-            CK(ctx->m2l_k32_s.ensure(2 * (size_t)nm), "alloc lists");
-            launch_expand_m2l<uint32_t>(ge, s, ctx->m2l.p, nm, shift, ctx->m2l_k32.p);
-            size_t tb = sort_keys_u32_temp(2 * nm, cbits);
-            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-            CK(sort_keys_u32(ctx->cub_tmp.p, tb, ctx->m2l_k32.p, ctx->m2l_k32_s.p, 2 * nm, cbits, s), "m2l sort");
-            launch_segments<uint32_t>(gs, s, ctx->m2l_k32_s.p, 2 * nm, shift, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p);
-        } else {
-            CK(ctx->m2l_keys.ensure(2 * (size_t)nm), "alloc lists");
-            CK(ctx->m2l_keys_s.ensure(2 * (size_t)nm), "alloc lists");
-            launch_expand_m2l<uint64_t>(ge, s, ctx->m2l.p, nm, shift, ctx->m2l_keys.p);
-            size_t tb = sort_keys_u64_temp(2 * nm, cbits);
-            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-            CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->m2l_keys.p, ctx->m2l_keys_s.p, 2 * nm, cbits, s), "m2l sort");
-            launch_segments<uint64_t>(gs, s, ctx->m2l_keys_s.p, 2 * nm, shift, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p);
-        }
-        CKL("m2l lists");
-    }
-    // P2P
-    const int np = ctx->n_p2p;
-    CK(ctx->p2p_seg_b.ensure(nc), "alloc lists");
-    CK(ctx->p2p_seg_e.ensure(nc), "alloc lists");
+    const int nm = ctx->n_m2l, np = ctx->n_p2p;
+    const size_t n_m2l_dir = 2 * (size_t)nm;
+    const size_t n_p2p_dir = np > 0 ? 2 * (size_t)np - (size_t)ctx->nleaves : 0;  // one entry per leaf self pair
+    if (n_m2l_dir > 0x7fffffffull || n_p2p_dir > 0x7fffffffull)
+        return fail(ctx, FMMX_OUT_OF_MEMORY, "interaction lists above 2^31 entries");
+    CK(ctx->m2l_off.ensure(nc + 1), "alloc lists");
+    CK(ctx->p2p_off.ensure(nc + 1), "alloc lists");
+    CK(ctx->list_cnt.ensure(nc + 1), "alloc lists");
+    CK(ctx->m2l_src_u.ensure(std::max<size_t>(n_m2l_dir, 1)), "alloc lists");
+    CK(ctx->m2l_src.ensure(std::max<size_t>(n_m2l_dir, 1)), "alloc lists");
+    // (room for 2 entries per pair: the scatter writes inside the counted
+    // segments whatever the number of self pairs)
+    CK(ctx->p2p_src_u.ensure(std::max<size_t>(2 * (size_t)np, 1)), "alloc lists");
+    CK(ctx->p2p_src.ensure(std::max<size_t>(2 * (size_t)np, 1)), "alloc lists");
     CK(ctx->inter.ensure(1), "alloc");
-    CK(cudaMemsetAsync(ctx->p2p_seg_b.p, 0, nc * sizeof(uint32_t), s), "memset");
-    CK(cudaMemsetAsync(ctx->p2p_seg_e.p, 0, nc * sizeof(uint32_t), s), "memset");
     CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
-    if (np > 0) {
-        const uint64_t sentinel = (uint64_t)nc << shift;  // above every valid key, within 2 * shift bits
-        LCOUNT(3);
-        const int nvalid = 2 * np - ctx->nleaves;
-        const unsigned ge = grid_for(np, 256), gs = grid_for(nvalid, 256);
-        if (k32) {
-            CK(ctx->p2p_k32.ensure(2 * (size_t)np), "alloc lists");
-            CK(ctx->p2p_k32_s.ensure(2 * (size_t)np), "alloc lists");
-            launch_expand_p2p<uint32_t>(ge, s, ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_k32.p,
-                                        ctx->inter.p);
-            size_t tb = sort_keys_u32_temp(2 * np, cbits);
-            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-            CK(sort_keys_u32(ctx->cub_tmp.p, tb, ctx->p2p_k32.p, ctx->p2p_k32_s.p, 2 * np, cbits, s), "p2p sort");
-            launch_segments<uint32_t>(gs, s, ctx->p2p_k32_s.p, nvalid, shift, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p);
-        } else {
-            CK(ctx->p2p_keys.ensure(2 * (size_t)np), "alloc lists");
-            CK(ctx->p2p_keys_s.ensure(2 * (size_t)np), "alloc lists");
-            launch_expand_p2p<uint64_t>(ge, s, ctx->p2p.p, np, shift, ctx->c_count.p, sentinel, ctx->p2p_keys.p,
-                                        ctx->inter.p);
-            size_t tb = sort_keys_u64_temp(2 * np, cbits);
-            CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-            CK(sort_keys_u64(ctx->cub_tmp.p, tb, ctx->p2p_keys.p, ctx->p2p_keys_s.p, 2 * np, cbits, s), "p2p sort");
-            launch_segments<uint64_t>(gs, s, ctx->p2p_keys_s.p, nvalid, shift, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p);
-        }
-        CKL("p2p lists");
+    const size_t tb = std::max(directed_list_temp((int)n_m2l_dir, nc), directed_list_temp((int)n_p2p_dir, nc));
+    CK(ctx->cub_tmp.ensure(tb), "alloc sort");
+    LCOUNT(12);  // per list: count, scan (2), scatter, segment sorts (2)
+    CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l.p, nm, (int)n_m2l_dir, nc, nullptr, nullptr,
+                           ctx->list_cnt.p, ctx->m2l_off.p, ctx->m2l_src_u.p, ctx->m2l_src.p, grid_for(nm, 256), s),
+       "m2l lists");
+    CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p.p, np, (int)n_p2p_dir, nc, ctx->c_count.p,
+                           ctx->inter.p, ctx->list_cnt.p, ctx->p2p_off.p, ctx->p2p_src_u.p, ctx->p2p_src.p,
+                           grid_for(np, 256), s),
+       "p2p lists");
+    CKL("lists");
+    if (ctx->cfg.precision == FMMX_MIXED) {
+        // near-field work units: per leaf ceil(sources / P2P_UNIT_SRC), and the
+        // scratch for the partial sums of leaves with several units
+        for (DBuf<uint32_t>* b : {&ctx->p2p_units, &ctx->p2p_scr, &ctx->p2p_uoff, &ctx->p2p_soff})
+            CK(b->ensure(nc + 1), "alloc lists");
+        CK(ctx->p2p_next.ensure(1), "alloc lists");
+        const DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
+        launch_p2p_plan(grid_for(nc + 1, 256), s, nc, lp, ctx->c_count.p, ctx->p2p_units.p, ctx->p2p_scr.p);
+        CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_units.p, ctx->p2p_uoff.p, nc + 1, s), "p2p units");
+        CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
+        LCOUNT(5);
+        uint32_t nscr = 0;
+        CK(cudaMemcpyAsync(&nscr, ctx->p2p_soff.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
+        CK(cudaStreamSynchronize(s), "p2p units");
+        CK(ctx->p2p_part.ensure(std::max<size_t>(nscr, 1)), "alloc p2p scratch");
     }
     return FMMX_OK;
 }
@@ -683,7 +661,9 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     // near field on the second stream, beside the far field
     if (tm) CK(cudaEventRecord(ev[12], s2), "event");
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)nc, s2, lp, nc, cv,
+    CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
+    const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_soff.p, ctx->p2p_part.p, ctx->p2p_next.p};
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)ctx->nsm * 8, s2, lp, nc, cv, units,
                      ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s2), "event");
@@ -701,7 +681,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
         CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, work, ctx->nsm, s), "m2l");
     }
     if (tm) CK(cudaEventRecord(ev[6], s), "event");
-    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 2);
+    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 3);  // m2l, l2l per level, p2p + combine, l2p
     for (int L = 1; L < ctx->nlevels; ++L) {
         const int cnt = ctx->lvl_count[L];
         const unsigned g = std::min<unsigned>(cnt, 148u * 16u);
@@ -829,11 +809,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     CK(cudaEventRecord(ctx->fork[1], s2), "event");
     CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L reads the lists
 
-    const bool k32 = ctx->keys32;
-    DirList lm{k32 ? nullptr : ctx->m2l_keys_s.p, k32 ? ctx->m2l_k32_s.p : nullptr, ctx->m2l_seg_b.p, ctx->m2l_seg_e.p,
-               ctx->list_shift};
-    DirList lp{k32 ? nullptr : ctx->p2p_keys_s.p, k32 ? ctx->p2p_k32_s.p : nullptr, ctx->p2p_seg_b.p, ctx->p2p_seg_e.p,
-               ctx->list_shift};
+    DirList lm{nullptr, ctx->m2l_src.p, ctx->m2l_off.p, ctx->m2l_off.p + 1, 32};
+    DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
     if (mixed) {
         fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot, tm);
         if (ms != FMMX_OK) return ms;

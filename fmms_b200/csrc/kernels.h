@@ -53,10 +53,10 @@ struct WalkBufs {
 };
 
 // Segmented directed interaction list: for destination cell c, sources
-// src[seg_begin[c] .. seg_end[c]) (ascending).
+// src(key(i)) for i in [seg_begin[c], seg_end[c]), in ascending order.
 struct DirList {
-    const uint64_t* keys;    // (dst << shift) | src, sorted; shift = bits of the cell count
-    const uint32_t* keys32;  // the same in 32 bits when 2 * shift <= 32 (then keys is null)
+    const uint64_t* keys;    // entries (dst << shift) | src, or null
+    const uint32_t* keys32;  // 32-bit entries (then keys is null); with shift = 32 the entries are the sources
     const uint32_t* seg_begin;
     const uint32_t* seg_end;
     int shift;
@@ -96,16 +96,17 @@ __global__ void k_fprepass(CellsView cells, const double* x, const double* y, co
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
 
 // lists.cu
-// Directed list keys from the walk's mutual pairs, with K = uint32_t or
-// uint64_t keys (launchers in lists.cu).
-template <typename K>
-void launch_expand_m2l(unsigned grid, cudaStream_t s, const uint2* pairs, int np, int shift, K* keys);
-template <typename K>
-void launch_expand_p2p(unsigned grid, cudaStream_t s, const uint2* pairs, int np, int shift, const uint32_t* count,
-                       uint64_t sentinel, K* keys, unsigned long long* interactions);
-template <typename K>
-void launch_segments(unsigned grid, cudaStream_t s, const K* keys, int nkeys, int shift, uint32_t* seg_begin,
-                     uint32_t* seg_end);
+// Directed list of `np` walk pairs with `nitems` directed entries: per
+// destination c its sources src[off[c] .. off[c+1]) in ascending order
+// (off has ncells + 1 entries; cnt is ncells + 1 scratch counters). With
+// body_count, also adds the directed body-body interactions (P2P).
+size_t directed_list_temp(int nitems, int ncells);
+// exclusive prefix sum of n values (temp storage as for directed_list_temp)
+cudaError_t scan_u32(void* tmp, size_t tmp_bytes, const uint32_t* in, uint32_t* out, int n, cudaStream_t s);
+cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs, int np, int nitems, int ncells,
+                                const uint32_t* body_count, unsigned long long* interactions, uint32_t* cnt,
+                                uint32_t* off, uint32_t* src_unsorted, uint32_t* src, unsigned grid,
+                                cudaStream_t s);
 
 // m2l.cu
 void upload_tables_m2l(const OrderTables& t, cudaStream_t s);
@@ -135,9 +136,21 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* body_leaf, const uint32_t* 
                             const double* ell, int p, const zf* loc, const double* x, const double* y,
                             const double* z, const double* nax, const double* nay, const double* naz,
                             const double* npot, double* acc, double* pot);
-void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, const double* x,
-                      const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
-                      double* az, double* pot);
+// Near-field work units: the sources of a leaf in units of P2P_UNIT_SRC
+// source leaves (uoff: units of cell c at uoff[c] .. uoff[c+1]; soff: the
+// partial sums of a leaf with several units at part[soff[c] + k * count + i]).
+#define P2P_UNIT_SRC 1024
+struct P2pUnits {
+    const uint32_t* uoff;  // ncells + 1
+    const uint32_t* soff;  // ncells + 1
+    double4* part;
+    unsigned* next;  // work counter, zero at launch
+};
+void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
+                     uint32_t* scratch);
+void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
+                      const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
+                      double* ay, double* az, double* pot);
 
 // p2p.cu
 __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,

@@ -406,13 +406,46 @@ __device__ __forceinline__ void p2p_term(const float4 s, float xi, float yi, flo
     pt += mi;
 }
 
+// Work units of the near field: the sources of leaf c are cut into units of
+// P2P_UNIT_SRC source leaves, units[c] = ceil(len / P2P_UNIT_SRC), so a leaf
+// in a dense cluster core with thousands of neighbours spreads over many
+// blocks instead of holding one block to the end of the launch (the
+// load-balancing aim of the reference's split_fat, crates/visual/src/
+// gpufmm.rs:1350-1414). A leaf with one unit writes its bodies' sums
+// directly; the units of a leaf with several write partial sums, which
+// k_p2p_combine adds per body in unit order (a fixed order: the results do
+// not depend on which block ran which unit).
+__global__ void k_p2p_plan(int ncells, DirList L, const uint32_t* __restrict__ count, uint32_t* __restrict__ units,
+                           uint32_t* __restrict__ scratch) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += gridDim.x * blockDim.x) {
+        uint32_t nu = 0;
+        if (c < ncells) {
+            const uint32_t len = L.seg_end[c] - L.seg_begin[c];
+            nu = (len + P2P_UNIT_SRC - 1) / P2P_UNIT_SRC;
+        }
+        units[c] = nu;
+        scratch[c] = nu > 1 ? nu * count[c] : 0;
+    }
+}
+
+__device__ __forceinline__ int unit_cell(const uint32_t* __restrict__ uoff, int ncells, uint32_t u) {
+    int lo = 0, hi = ncells;  // the last c with uoff[c] <= u
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (uoff[mid] <= u) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // TILE: source bodies staged per shared-memory tile (the tile shape the
 // autotuner picks). Each thread carries two targets, so every staged source
 // feeds two interactions; groups of G threads cover the leaf's targets and
 // R = BLOCK / G groups split each tile. The target's own slot is skipped by
-// position only in the tiles that overlap the target leaf itself.
+// position only in the tiles that overlap the target leaf itself. Blocks are
+// persistent and take units from a counter.
 template <int P2PM_TILE>
-__global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv,
+__global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv, P2pUnits U,
                                                          const double* __restrict__ x, const double* __restrict__ y,
                                                          const double* __restrict__ z, const double* __restrict__ m,
                                                          float soft2, double* __restrict__ ax,
@@ -423,12 +456,21 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
     __shared__ uint32_t sfirst[P2PM_SRC_CHUNK];
     __shared__ uint32_t wsum[P2PM_BLOCK / 32];
     __shared__ int self_pos;
+    __shared__ uint32_t unit_sh;
     __shared__ float red[16][P2PM_BLOCK];
     const int tid = threadIdx.x;
     const int lane = tid & 31, wid = tid >> 5;
-    for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
-        const uint32_t beg = L.seg_begin[c], end = L.seg_end[c];
-        if (beg >= end) continue;
+    const uint32_t nunits = U.uoff[ncells];
+    for (;;) {
+        if (tid == 0) unit_sh = atomicAdd(U.next, 1u);
+        __syncthreads();
+        const uint32_t u = unit_sh;
+        __syncthreads();
+        if (u >= nunits) break;
+        const int c = unit_cell(U.uoff, ncells, u);
+        const uint32_t k = u - U.uoff[c], nu = U.uoff[c + 1] - U.uoff[c];
+        const uint32_t beg = L.seg_begin[c] + k * P2P_UNIT_SRC;
+        const uint32_t end = min(L.seg_end[c], beg + P2P_UNIT_SRC);
         const double cx = cv.cx[c], cy = cv.cy[c], cz = cv.cz[c];
         const uint32_t tf = cv.first[c], tn = cv.count[c];
         for (uint32_t t0 = 0; t0 < tn; t0 += 2 * P2PM_BLOCK) {
@@ -541,29 +583,67 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                 double sacc[4] = {0, 0, 0, 0};
                 for (int r = 0; r < R; ++r) {
                     const int q = r * G + gi;
-                    for (int k = 0; k < 4; ++k)
-                        sacc[k] += (double)red[8 * half + 2 * k][q] + (double)red[8 * half + 2 * k + 1][q];
+                    for (int k4 = 0; k4 < 4; ++k4)
+                        sacc[k4] += (double)red[8 * half + 2 * k4][q] + (double)red[8 * half + 2 * k4 + 1][q];
                 }
-                const uint32_t slot = tf + t0 + tid;
-                ax[slot] = sacc[0];
-                ay[slot] = sacc[1];
-                az[slot] = sacc[2];
-                pot[slot] = sacc[3];
+                if (nu == 1) {
+                    const uint32_t slot = tf + t0 + tid;
+                    ax[slot] = sacc[0];
+                    ay[slot] = sacc[1];
+                    az[slot] = sacc[2];
+                    pot[slot] = sacc[3];
+                } else {
+                    U.part[U.soff[c] + k * tn + t0 + tid] = make_double4(sacc[0], sacc[1], sacc[2], sacc[3]);
+                }
             }
             __syncthreads();
         }
     }
 }
 
-void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, const double* x,
-                      const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
-                      double* az, double* pot) {
+// The bodies of the leaves with several units: the units' partial sums, in
+// unit order (one warp per leaf).
+__global__ void k_p2p_combine(int ncells, CellsView cv, P2pUnits U, double* __restrict__ ax, double* __restrict__ ay,
+                              double* __restrict__ az, double* __restrict__ pot) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
+        const uint32_t nu = U.uoff[c + 1] - U.uoff[c];
+        if (nu <= 1) continue;
+        const uint32_t tn = cv.count[c], tf = cv.first[c];
+        const double4* pp = U.part + U.soff[c];
+        for (uint32_t i = lane; i < tn; i += 32) {
+            double4 s = pp[i];
+            for (uint32_t k = 1; k < nu; ++k) {
+                const double4 v = pp[k * tn + i];
+                s.x += v.x;
+                s.y += v.y;
+                s.z += v.z;
+                s.w += v.w;
+            }
+            ax[tf + i] = s.x;
+            ay[tf + i] = s.y;
+            az[tf + i] = s.z;
+            pot[tf + i] = s.w;
+        }
+    }
+}
+
+void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
+                     uint32_t* scratch) {
+    k_p2p_plan<<<grid, 256, 0, s>>>(ncells, L, count, units, scratch);
+}
+
+void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
+                      const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
+                      double* ay, double* az, double* pot) {
     if (tile <= 128)
-        k_p2p_mixed<128><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
+        k_p2p_mixed<128><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
     else if (tile <= 256)
-        k_p2p_mixed<256><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
+        k_p2p_mixed<256><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
     else
-        k_p2p_mixed<512><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, x, y, z, m, soft2, ax, ay, az, pot);
+        k_p2p_mixed<512><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+    k_p2p_combine<<<grid_for((size_t)ncells * 32, 256), 256, 0, s>>>(ncells, cv, U, ax, ay, az, pot);
 }
 
 }  // namespace fmmx

@@ -1,5 +1,5 @@
-// Radix sorts used by the engine (Morton keys, depth-first renumbering and the
-// directed interaction lists), via CUB's device radix sort. LSD radix sort is
+// Radix sorts used by the engine (Morton keys and the depth-first
+// renumbering), via CUB's device radix sort. LSD radix sort is
 // stable, so equal Morton keys keep ascending particle index: the tie rule of
 // a stable sort_by_key (the reference's sort_unstable_by_key, tree.rs:130,
 // leaves ties unspecified).
@@ -20,28 +20,6 @@ size_t sort_pairs_u64_u32_temp(int n, int end_bit) {
 cudaError_t sort_pairs_u64_u32(void* tmp, size_t tmp_bytes, const uint64_t* kin, uint64_t* kout, const uint32_t* vin,
                                uint32_t* vout, int n, int end_bit, cudaStream_t s) {
     return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kin, kout, vin, vout, n, 0, end_bit, s);
-}
-
-size_t sort_keys_u64_temp(int n, int end_bit) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr, n, 0, end_bit);
-    return bytes;
-}
-
-cudaError_t sort_keys_u64(void* tmp, size_t tmp_bytes, const uint64_t* kin, uint64_t* kout, int n, int end_bit,
-                          cudaStream_t s) {
-    return cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, n, 0, end_bit, s);
-}
-
-size_t sort_keys_u32_temp(int n, int end_bit) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, n, 0, end_bit);
-    return bytes;
-}
-
-cudaError_t sort_keys_u32(void* tmp, size_t tmp_bytes, const uint32_t* kin, uint32_t* kout, int n, int end_bit,
-                          cudaStream_t s) {
-    return cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, n, 0, end_bit, s);
 }
 
 // Independent sorts of the segments [off[s], off[s+1]) (a forest of systems).

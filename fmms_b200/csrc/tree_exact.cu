@@ -750,14 +750,6 @@ __device__ __forceinline__ bool accept_dehnen(const CellsView& cv, const MacPara
     return est * ma / r2 < mp.eps * fminv[b];
 }
 
-// Geometric opening angle (extension): (rho_A + rho_B) / r < theta.
-__device__ __forceinline__ bool accept_theta(const CellsView& cv, const MacParams& mp, int a, int b) {
-    const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double sum_rho = cv.rho[a] + cv.rho[b];
-    return sum_rho < mp.theta * sqrt(r2);
-}
-
 // Separation condition (extension, with softening): the bodies of the two
 // cells are at least mp.gap apart, r - rho_A - rho_B >= gap.
 __device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp, int a, int b) {
@@ -765,6 +757,21 @@ __device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp,
     const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
     const double r2 = dx * dx + dy * dy + dz * dz;
     return sqrt(r2) - (cv.rho[a] + cv.rho[b]) >= mp.gap;
+}
+
+// The geometric MAC (extension): accept when (rho_A + rho_B) < theta r, both
+// ways round as the reference's walk applies its MAC (walk.rs:138-139), and
+// gap_ok. The
+// two directions and gap_ok evaluate the same r2 (the squares of b - a and
+// a - b are equal bit for bit) and the same rho sum (addition commutes), so
+// one square root decides all three.
+__device__ __forceinline__ bool accept_theta_pair(const CellsView& cv, const MacParams& mp, int a, int b) {
+    const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double sum_rho = cv.rho[a] + cv.rho[b];
+    const double r = sqrt(r2);
+    if (!(sum_rho < mp.theta * r)) return false;
+    return !(mp.gap > 0.0) || r - sum_rho >= mp.gap;
 }
 
 // ------------------------------------------------------------ dual walk
@@ -821,10 +828,10 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
             } else {
                 bool acc;
                 if (mp.mode == FMMX_MAC_DEHNEN)
-                    acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a);
+                    acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a) &&
+                          gap_ok(cv, mp, a, b);
                 else
-                    acc = accept_theta(cv, mp, a, b) && accept_theta(cv, mp, b, a);
-                acc = acc && gap_ok(cv, mp, a, b);
+                    acc = accept_theta_pair(cv, mp, a, b);
                 if (acc) {
                     kind = WK_M2L;
                 } else if (la && lb) {
