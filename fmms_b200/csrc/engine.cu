@@ -621,7 +621,7 @@ fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
     CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
     const size_t tb = std::max(directed_list_temp((int)n_m2l_dir, nc), directed_list_temp((int)n_p2p_dir, nc));
     CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-    LCOUNT(12);  // per list: count, scan (2), scatter, segment sorts (2)
+    LCOUNT(14);  // per list: count, scan (2), scatter, segment sorts (3)
     CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l.p, nm, (int)n_m2l_dir, nc, nullptr, nullptr,
                            ctx->list_cnt.p, ctx->m2l_off.p, ctx->m2l_src_u.p, ctx->m2l_src.p, grid_for(nm, 256), s),
        "m2l lists");

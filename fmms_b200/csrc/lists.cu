@@ -8,7 +8,7 @@
 // destination -- count the entries per destination, scan the counts into
 // segment offsets, scatter every source into its destination's segment --
 // followed by a sort of each segment's sources (a bitonic network per
-// segment, in shared memory). The entries of destination c
+// segment, in registers). The entries of destination c
 // are then its sources in ascending order, src[off[c] .. off[c+1]), whatever
 // order the walk's atomics appended the pairs in, which fixes the
 // accumulation order and so every result bit.
@@ -51,88 +51,209 @@ __global__ void k_scatter_dst(const uint2* __restrict__ pairs, int np, const uin
     }
 }
 
-// Ascending sort of a[0..n) by a bitonic network over P = 2^k >= n slots in
-// which every comparator puts the smaller value at the lower index (the first
-// step of each merge compares mirrored positions, the others i with i + h).
-// Slots n..P-1 act as +infinity: a comparator whose upper slot is one of them
-// never swaps, so they are never read or written. All threads of the block
-// call it; `a` is shared or global memory of this block only.
-__device__ void bitonic_sort_block(uint32_t* a, int n) {
-    int P = 1;
-    while (P < n) P <<= 1;
-    for (int size = 2; size <= P; size <<= 1) {
-        const int hs = size >> 1;
-        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-            const int i = (t / hs) * size + (t % hs);
-            const int j = (t / hs) * size + size - 1 - (t % hs);
-            if (j < n) {
-                const uint32_t x = a[i], y = a[j];
-                if (x > y) {
-                    a[i] = y;
-                    a[j] = x;
-                }
-            }
-        }
-        __syncthreads();
-        for (int h = hs >> 1; h > 0; h >>= 1) {
-            for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                const int i = (t / h) * 2 * h + (t % h);
-                const int j = i + h;
-                if (j < n) {
-                    const uint32_t x = a[i], y = a[j];
-                    if (x > y) {
-                        a[i] = y;
-                        a[j] = x;
-                    }
-                }
-            }
-            __syncthreads();
+// ---------------------------------------------------------------- segment sort
+// Ascending sorts by a bitonic network in which every comparator puts the
+// smaller value at the lower index: merge stage `size` starts with a mirror
+// step (e against e ^ (size - 1)) and continues with half-cleaners (e
+// against e ^ h, h = size/4 .. 1). A warp holds a chunk of 32 R elements,
+// element e = lane * R + j in register v[j]: steps with h < R are register
+// compares, the others shuffles between lanes. Slots past the segment hold
+// 0xffffffff (never a cell id), so they sort to the end.
+__device__ __forceinline__ void cmp_up(uint32_t& lo, uint32_t& hi) {
+    const uint32_t a = min(lo, hi), b = max(lo, hi);
+    lo = a;
+    hi = b;
+}
+
+// Every step distance is a template argument, so the register array is
+// indexed by constants only (no local-memory copy of it).
+// half-cleaner at distance H within the warp's chunk
+template <int R, int H>
+__device__ __forceinline__ void warp_half(uint32_t (&v)[R], int lane) {
+    if constexpr (H < R) {
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+            if ((j & H) == 0) cmp_up(v[j], v[j | H]);
+    } else {
+        constexpr int lm = H / R;
+        const bool low = (lane & lm) == 0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v[j], lm);
+            v[j] = low ? min(v[j], o) : max(v[j], o);
         }
     }
 }
 
-#define SEG_SMALL 2048
-#define SEG_LARGE_SMEM 32768
+// half-cleaners H, H/2, .., 1
+template <int R, int H>
+__device__ __forceinline__ void warp_clean(uint32_t (&v)[R], int lane) {
+    warp_half<R, H>(v, lane);
+    if constexpr (H > 1) warp_clean<R, H / 2>(v, lane);
+}
 
-// One block per destination: segments of up to SEG_SMALL entries are sorted in
-// shared memory into `out`; longer ones are appended to `big` for
-// k_sort_segments_large.
+// mirror step of merge stage SIZE (SIZE <= 32 R)
+template <int R, int SIZE>
+__device__ __forceinline__ void warp_mirror(uint32_t (&v)[R], int lane) {
+    if constexpr (SIZE <= R) {
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+            if (j < (j ^ (SIZE - 1))) cmp_up(v[j], v[j ^ (SIZE - 1)]);
+    } else {
+        constexpr int lm = SIZE / R - 1;
+        const bool low = (lane & (SIZE / R / 2)) == 0;
+        uint32_t o[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) o[j] = __shfl_xor_sync(0xffffffffu, v[R - 1 - j], lm);
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = low ? min(v[j], o[j]) : max(v[j], o[j]);
+    }
+}
+
+// merge stages SIZE .. 32 R: the full sort of the warp's 32 R elements from SIZE = 2
+template <int R, int SIZE = 2>
+__device__ __forceinline__ void warp_sort(uint32_t (&v)[R], int lane) {
+    warp_mirror<R, SIZE>(v, lane);
+    if constexpr (SIZE >= 4) warp_clean<R, SIZE / 4>(v, lane);
+    if constexpr (SIZE < 32 * R) warp_sort<R, 2 * SIZE>(v, lane);
+}
+
+// the half-cleaners h = 512 .. 1 of a merge stage, on a 1024-element chunk
+__device__ __forceinline__ void warp_clean_1024(uint32_t (&v)[32], int lane) { warp_clean<32, 512>(v, lane); }
+
+template <int R>
+__device__ __forceinline__ void warp_sort_segment(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n,
+                                                  int lane) {
+    uint32_t v[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const int e = lane * R + j;
+        v[j] = e < n ? in[e] : 0xffffffffu;
+    }
+    warp_sort<R>(v, lane);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const int e = lane * R + j;
+        if (e < n) out[e] = v[j];
+    }
+}
+
+#define SEG_WARP 1024
+#define SEG_MID 4096  // 1024 < n <= SEG_MID: blocks of 4 warps, the segment in 16 KB of shared memory;
+                      // longer: blocks of 8 warps in place in `out` (the segment stays in L2), many per SM
+
+// One warp per destination: segments of up to SEG_WARP entries are sorted in
+// registers into `out`; longer ones are appended to `mid` (up to SEG_MID) or
+// `big` for the block kernels.
 __global__ void __launch_bounds__(256) k_sort_segments(const uint32_t* __restrict__ off, int nseg,
                                                        const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                       int* __restrict__ mid, int* __restrict__ nmid,
                                                        int* __restrict__ big, int* __restrict__ nbig) {
-    __shared__ uint32_t buf[SEG_SMALL];
-    const int c = blockIdx.x;
-    if (c >= nseg) return;
-    const uint32_t b = off[c];
-    const int n = (int)(off[c + 1] - b);
-    if (n == 0) return;
-    if (n > SEG_SMALL) {
-        if (threadIdx.x == 0) big[atomicAdd(nbig, 1)] = c;
-        return;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nseg; c += warps) {
+        const uint32_t b = off[c];
+        const int n = (int)(off[c + 1] - b);
+        if (n == 0) continue;
+        if (n > SEG_WARP) {
+            if (lane == 0) {
+                if (n <= SEG_MID) mid[atomicAdd(nmid, 1)] = c;
+                else big[atomicAdd(nbig, 1)] = c;
+            }
+            continue;
+        }
+        const uint32_t* src = in + b;
+        uint32_t* dst = out + b;
+        if (n <= 32) warp_sort_segment<1>(src, dst, n, lane);
+        else if (n <= 64) warp_sort_segment<2>(src, dst, n, lane);
+        else if (n <= 128) warp_sort_segment<4>(src, dst, n, lane);
+        else if (n <= 256) warp_sort_segment<8>(src, dst, n, lane);
+        else if (n <= 512) warp_sort_segment<16>(src, dst, n, lane);
+        else warp_sort_segment<32>(src, dst, n, lane);
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = in[b + i];
-    __syncthreads();
-    if (n > 1) bitonic_sort_block(buf, n);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) out[b + i] = buf[i];
 }
 
-// The longer segments (a few fat leaves with thousands of neighbours): in
-// shared memory up to SEG_LARGE_SMEM entries, in place in `out` beyond.
-__global__ void __launch_bounds__(1024) k_sort_segments_large(const uint32_t* __restrict__ off,
-                                                              const uint32_t* __restrict__ in,
-                                                              uint32_t* __restrict__ out, const int* __restrict__ big,
-                                                              const int* __restrict__ nbig) {
+// The longer segments (leaves in dense cluster cores with thousands of
+// neighbours), one block each: every warp sorts 1024-element chunks in
+// registers; the merge stages above 1024 run their steps across chunks
+// (distance >= 1024) on the whole segment, block-synchronised, and the steps
+// within chunks again in registers. The segment is in shared memory up to
+// SMEM_ENTRIES entries, in place in `out` beyond; slots from n up to the
+// power of two are virtual (+infinity: never read or written).
+template <int THREADS, int SMEM_ENTRIES>
+__global__ void __launch_bounds__(THREADS) k_sort_segments_large(const uint32_t* __restrict__ off,
+                                                                 const uint32_t* __restrict__ in,
+                                                                 uint32_t* __restrict__ out,
+                                                                 const int* __restrict__ big,
+                                                                 const int* __restrict__ nbig) {
     extern __shared__ uint32_t sbuf[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = THREADS >> 5;
     const int nb = *nbig;
     for (int q = blockIdx.x; q < nb; q += gridDim.x) {
         const int c = big[q];
         const uint32_t b = off[c];
         const int n = (int)(off[c + 1] - b);
-        uint32_t* a = n <= SEG_LARGE_SMEM ? sbuf : out + b;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = in[b + i];
+        uint32_t* a = n <= SMEM_ENTRIES ? sbuf : out + b;
+        int P = SEG_WARP;
+        while (P < n) P <<= 1;
+        const int nchunk = P / SEG_WARP;
+        // chunks sorted in registers
+        for (int ch = wid; ch < nchunk; ch += nw) {
+            uint32_t v[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int e = ch * SEG_WARP + lane * 32 + j;
+                v[j] = e < n ? in[b + e] : 0xffffffffu;
+            }
+            warp_sort<32>(v, lane);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int e = ch * SEG_WARP + lane * 32 + j;
+                if (e < n) a[e] = v[j];
+            }
+        }
         __syncthreads();
-        bitonic_sort_block(a, n);
-        if (n <= SEG_LARGE_SMEM)
+        for (int size = 2 * SEG_WARP; size <= P; size <<= 1) {
+            // steps across chunks: the mirror step, then half-cleaners h >= 1024
+            for (int h = size / 2; h >= SEG_WARP; h >>= 1) {
+                const bool mirror = h == size / 2;
+                for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                    int i, j;
+                    if (mirror) {
+                        i = (t / h) * size + (t % h);
+                        j = (t / h) * size + size - 1 - (t % h);
+                    } else {
+                        i = (t / h) * 2 * h + (t % h);
+                        j = i + h;
+                    }
+                    if (j < n) {
+                        const uint32_t x = a[i], y = a[j];
+                        if (x > y) {
+                            a[i] = y;
+                            a[j] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            // the remaining half-cleaners stay within chunks
+            for (int ch = wid; ch < nchunk; ch += nw) {
+                uint32_t v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int e = ch * SEG_WARP + lane * 32 + j;
+                    v[j] = e < n ? a[e] : 0xffffffffu;
+                }
+                warp_clean_1024(v, lane);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int e = ch * SEG_WARP + lane * 32 + j;
+                    if (e < n) a[e] = v[j];
+                }
+            }
+            __syncthreads();
+        }
+        if (n <= SMEM_ENTRIES)
             for (int i = threadIdx.x; i < n; i += blockDim.x) out[b + i] = a[i];
         __syncthreads();
     }
@@ -146,8 +267,8 @@ size_t directed_list_temp(int nitems, int ncells) {
     (void)nitems;
     size_t a = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, a, (const uint32_t*)nullptr, (uint32_t*)nullptr, ncells + 1);
-    // after the scan's storage: the count and the ids of the long segments
-    return ((a + 255) / 256) * 256 + sizeof(int) * ((size_t)ncells + 64);
+    // after the scan's storage: the counts and the ids of the long segments
+    return ((a + 255) / 256) * 256 + sizeof(int) * (2 * (size_t)ncells + 128);
 }
 
 cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs, int np, int nitems, int ncells,
@@ -158,22 +279,24 @@ cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs,
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt, off, ncells + 1, s);
     const size_t big_at = ((scan_bytes + 255) / 256) * 256;
-    if (tmp_bytes < big_at + sizeof(int) * ((size_t)ncells + 64)) return cudaErrorInvalidValue;
-    int* nbig = reinterpret_cast<int*>(static_cast<char*>(tmp) + big_at);
-    int* big = nbig + 64;
+    if (tmp_bytes < big_at + sizeof(int) * (2 * (size_t)ncells + 128)) return cudaErrorInvalidValue;
+    int* nbig = reinterpret_cast<int*>(static_cast<char*>(tmp) + big_at);  // [0] long, [32] middle
+    int* nmid = nbig + 32;
+    int* big = nbig + 128;
+    int* mid = big + ncells;
     cudaError_t e = cudaMemsetAsync(cnt, 0, (size_t)(ncells + 1) * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     if (np > 0) k_count_dst<<<grid, 256, 0, s>>>(pairs, np, cnt, body_count, interactions);
     e = cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, cnt, off, ncells + 1, s);
     if (e != cudaSuccess || np == 0) return e;
     k_scatter_dst<<<grid, 256, 0, s>>>(pairs, np, off, cnt, src_unsorted);
-    e = cudaMemsetAsync(nbig, 0, sizeof(int), s);
+    e = cudaMemsetAsync(nbig, 0, 128 * sizeof(int), s);
     if (e != cudaSuccess) return e;
-    k_sort_segments<<<ncells, 256, 0, s>>>(off, ncells, src_unsorted, src, big, nbig);
-    e = cudaFuncSetAttribute(k_sort_segments_large, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SEG_LARGE_SMEM * (int)sizeof(uint32_t));  // 128 KB, on the current device
-    if (e != cudaSuccess) return e;
-    k_sort_segments_large<<<148, 1024, SEG_LARGE_SMEM * sizeof(uint32_t), s>>>(off, src_unsorted, src, big, nbig);
+    k_sort_segments<<<grid_for((size_t)ncells * 32, 256, 148u * 64u), 256, 0, s>>>(off, ncells, src_unsorted, src,
+                                                                                   mid, nmid, big, nbig);
+    k_sort_segments_large<128, SEG_MID><<<148 * 12, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src, mid,
+                                                                                          nmid);
+    k_sort_segments_large<256, 0><<<148 * 8, 256, 0, s>>>(off, src_unsorted, src, big, nbig);
     return cudaGetLastError();
 }
 
