@@ -90,6 +90,7 @@ struct CellsView {
     const double* cz;
     const double* mass;
     const double* rho;
+    const double4* geo;  // cx, cy, cz, rho of each cell in one 32-byte record (the walk's loads)
 };
 
 static inline unsigned grid_for(size_t n, int block, unsigned cap = 148u * 32u) {

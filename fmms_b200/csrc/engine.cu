@@ -139,6 +139,7 @@ struct fmmx_ctx {
     DBuf<int32_t> c_child, c_parent, level_cells, body_leaf;
     DBuf<uint8_t> c_leaf, c_level;
     DBuf<double> c_cx, c_cy, c_cz, c_mass, c_rho;
+    DBuf<double4> c_geo;  // (cx, cy, cz, rho) per cell
 
     // expansions
     DBuf<zd> moments, locals;
@@ -158,6 +159,8 @@ struct fmmx_ctx {
     // per destination cell c: sources src[off[c] .. off[c+1]), ascending
     DBuf<uint32_t> m2l_src_u, m2l_src, p2p_src_u, p2p_src;  // scattered, then sorted within segments
     DBuf<uint32_t> m2l_off, p2p_off, list_cnt;               // nc + 1 each
+    DBuf<int> m2l_longs, p2p_longs;                         // long-segment lists, 2 nc + 128 each
+    DBuf<uint32_t> long_bounds;
     // near-field work units of the mixed P2P (per leaf: units, scratch bodies)
     DBuf<uint32_t> p2p_units, p2p_scr, p2p_uoff, p2p_soff;
     DBuf<double4> p2p_part;
@@ -212,6 +215,7 @@ CellsView view(fmmx_ctx* c) {
     v.cz = c->c_cz.p;
     v.mass = c->c_mass.p;
     v.rho = c->c_rho.p;
+    v.geo = c->c_geo.p;
     return v;
 }
 
@@ -510,7 +514,9 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
         k_cell_h<<<grid_for(cnt, 256), 256, 0, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, ctx->c_parent.p,
                                                     ctx->box.p, ctx->c_h.p);
     }
-    LCOUNT(nlev);
+    CK(ctx->c_geo.ensure(nc), "alloc cells");
+    k_pack_geo<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_cx.p, ctx->c_cy.p, ctx->c_cz.p, ctx->c_rho.p, ctx->c_geo.p);
+    LCOUNT(nlev + 1);
     CKL("cell sizes");
     if (ctx->events) CK(cudaEventRecord(ctx->ev[1], s), "event");
     CK(cudaStreamSynchronize(s), "build");
@@ -621,16 +627,20 @@ fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
     CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
     const size_t tb = std::max(directed_list_temp((int)n_m2l_dir, nc), directed_list_temp((int)n_p2p_dir, nc));
     CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-    LCOUNT(14);  // per list: count, scan (2), scatter, segment sorts (3)
+    CK(ctx->m2l_longs.ensure(2 * (size_t)nc + 128), "alloc lists");
+    CK(ctx->p2p_longs.ensure(2 * (size_t)nc + 128), "alloc lists");
+    LCOUNT(12);  // per list: count, scan (2), scatter, segment sorts (2)
     CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l.p, nm, (int)n_m2l_dir, nc, nullptr, nullptr,
-                           ctx->list_cnt.p, ctx->m2l_off.p, ctx->m2l_src_u.p, ctx->m2l_src.p, grid_for(nm, 256), s),
+                           ctx->list_cnt.p, ctx->m2l_off.p, ctx->m2l_src_u.p, ctx->m2l_src.p, ctx->m2l_longs.p,
+                           grid_for(nm, 256), s),
        "m2l lists");
     CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p.p, np, (int)n_p2p_dir, nc, ctx->c_count.p,
                            ctx->inter.p, ctx->list_cnt.p, ctx->p2p_off.p, ctx->p2p_src_u.p, ctx->p2p_src.p,
-                           grid_for(np, 256), s),
+                           ctx->p2p_longs.p, grid_for(np, 256), s),
        "p2p lists");
     CKL("lists");
-    if (ctx->cfg.precision == FMMX_MIXED) {
+    const bool mixed = ctx->cfg.precision == FMMX_MIXED;
+    if (mixed) {
         // near-field work units: per leaf ceil(sources / P2P_UNIT_SRC), and the
         // scratch for the partial sums of leaves with several units
         for (DBuf<uint32_t>* b : {&ctx->p2p_units, &ctx->p2p_scr, &ctx->p2p_uoff, &ctx->p2p_soff})
@@ -641,10 +651,28 @@ fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
         CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_units.p, ctx->p2p_uoff.p, nc + 1, s), "p2p units");
         CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
         LCOUNT(5);
-        uint32_t nscr = 0;
-        CK(cudaMemcpyAsync(&nscr, ctx->p2p_soff.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
-        CK(cudaStreamSynchronize(s), "p2p units");
-        CK(ctx->p2p_part.ensure(std::max<size_t>(nscr, 1)), "alloc p2p scratch");
+    }
+    // host read-back: the number of long segments of each list and the P2P scratch size
+    int nlong_m = 0, nlong_p = 0;
+    uint32_t nscr = 0;
+    CK(cudaMemcpyAsync(&nlong_m, ctx->m2l_longs.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+    CK(cudaMemcpyAsync(&nlong_p, ctx->p2p_longs.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+    if (mixed) CK(cudaMemcpyAsync(&nscr, ctx->p2p_soff.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
+    CK(cudaStreamSynchronize(s), "lists");
+    if (mixed) CK(ctx->p2p_part.ensure(std::max<size_t>(nscr, 1)), "alloc p2p scratch");
+    if (nlong_m + nlong_p > 0) {
+        const int end_bit = bits_for((uint64_t)nc);
+        CK(ctx->long_bounds.ensure(2 * (size_t)std::max(nlong_m, nlong_p)), "alloc lists");
+        const size_t lt = std::max(long_segments_temp((int)n_m2l_dir, nlong_m, end_bit),
+                                   long_segments_temp((int)n_p2p_dir, nlong_p, end_bit));
+        CK(ctx->cub_tmp.ensure(lt), "alloc sort");
+        LCOUNT(2 * ((nlong_m > 0) + (nlong_p > 0)));
+        CK(sort_long_segments(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l_off.p, ctx->m2l_longs.p, nlong_m,
+                              ctx->m2l_src_u.p, ctx->m2l_src.p, (int)n_m2l_dir, end_bit, ctx->long_bounds.p, s),
+           "m2l lists");
+        CK(sort_long_segments(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_off.p, ctx->p2p_longs.p, nlong_p,
+                              ctx->p2p_src_u.p, ctx->p2p_src.p, (int)n_p2p_dir, end_bit, ctx->long_bounds.p, s),
+           "p2p lists");
     }
     return FMMX_OK;
 }
@@ -663,7 +691,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
     CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
     const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_soff.p, ctx->p2p_part.p, ctx->p2p_next.p};
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, (unsigned)ctx->nsm * 8, s2, lp, nc, cv, units,
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, ctx->nsm, s2, lp, nc, cv, units,
                      ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s2), "event");

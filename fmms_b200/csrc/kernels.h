@@ -94,19 +94,28 @@ __global__ void k_upward_exact(const int32_t* level_cells, int lstart, int lcnt,
 __global__ void k_fprepass(CellsView cells, const double* x, const double* y, const double* z, const double* m,
                            size_t n, const uint64_t* off, int nsys, const int32_t* roots, double* f, int* err);
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
+__global__ void k_pack_geo(int nc, const double* cx, const double* cy, const double* cz, const double* rho,
+                           double4* geo);
 
 // lists.cu
 // Directed list of `np` walk pairs with `nitems` directed entries: per
 // destination c its sources src[off[c] .. off[c+1]) in ascending order
 // (off has ncells + 1 entries; cnt is ncells + 1 scratch counters). With
-// body_count, also adds the directed body-body interactions (P2P).
+// body_count, also adds the directed body-body interactions (P2P). Segments
+// longer than 4096 entries are left for sort_long_segments: `longs`
+// (2 ncells + 128 ints) receives their count at [0] and ids from [128].
 size_t directed_list_temp(int nitems, int ncells);
-// exclusive prefix sum of n values (temp storage as for directed_list_temp)
-cudaError_t scan_u32(void* tmp, size_t tmp_bytes, const uint32_t* in, uint32_t* out, int n, cudaStream_t s);
 cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs, int np, int nitems, int ncells,
                                 const uint32_t* body_count, unsigned long long* interactions, uint32_t* cnt,
-                                uint32_t* off, uint32_t* src_unsorted, uint32_t* src, unsigned grid,
+                                uint32_t* off, uint32_t* src_unsorted, uint32_t* src, int* longs, unsigned grid,
                                 cudaStream_t s);
+size_t long_segments_temp(int nitems, int nlong, int end_bit);
+// the nlong long segments (count read back from longs[0]); bounds: 2 nlong scratch
+cudaError_t sort_long_segments(void* tmp, size_t tmp_bytes, const uint32_t* off, const int* longs, int nlong,
+                               const uint32_t* src_unsorted, uint32_t* src, int nitems, int end_bit, uint32_t* bounds,
+                               cudaStream_t s);
+// exclusive prefix sum of n values (temp storage as for directed_list_temp)
+cudaError_t scan_u32(void* tmp, size_t tmp_bytes, const uint32_t* in, uint32_t* out, int n, cudaStream_t s);
 
 // m2l.cu
 void upload_tables_m2l(const OrderTables& t, cudaStream_t s);
@@ -148,7 +157,7 @@ struct P2pUnits {
 };
 void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
                      uint32_t* scratch);
-void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
+void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
                       const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
                       double* ay, double* az, double* pot);
 

@@ -13,6 +13,7 @@
 // order the walk's atomics appended the pairs in, which fixes the
 // accumulation order and so every result bit.
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_radix_sort.cuh>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -140,7 +141,7 @@ __device__ __forceinline__ void warp_sort_segment(const uint32_t* __restrict__ i
 
 #define SEG_WARP 1024
 #define SEG_MID 4096  // 1024 < n <= SEG_MID: blocks of 4 warps, the segment in 16 KB of shared memory;
-                      // longer: blocks of 8 warps in place in `out` (the segment stays in L2), many per SM
+                      // longer: CUB's segmented radix sort, one block per segment (sort_long_segments)
 
 // One warp per destination: segments of up to SEG_WARP entries are sorted in
 // registers into `out`; longer ones are appended to `mid` (up to SEG_MID) or
@@ -267,37 +268,59 @@ size_t directed_list_temp(int nitems, int ncells) {
     (void)nitems;
     size_t a = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, a, (const uint32_t*)nullptr, (uint32_t*)nullptr, ncells + 1);
-    // after the scan's storage: the counts and the ids of the long segments
-    return ((a + 255) / 256) * 256 + sizeof(int) * (2 * (size_t)ncells + 128);
+    return a;
 }
 
 cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs, int np, int nitems, int ncells,
                                 const uint32_t* body_count, unsigned long long* interactions, uint32_t* cnt,
-                                uint32_t* off, uint32_t* src_unsorted, uint32_t* src, unsigned grid,
+                                uint32_t* off, uint32_t* src_unsorted, uint32_t* src, int* longs, unsigned grid,
                                 cudaStream_t s) {
     (void)nitems;
-    size_t scan_bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt, off, ncells + 1, s);
-    const size_t big_at = ((scan_bytes + 255) / 256) * 256;
-    if (tmp_bytes < big_at + sizeof(int) * (2 * (size_t)ncells + 128)) return cudaErrorInvalidValue;
-    int* nbig = reinterpret_cast<int*>(static_cast<char*>(tmp) + big_at);  // [0] long, [32] middle
-    int* nmid = nbig + 32;
-    int* big = nbig + 128;
+    int* nbig = longs;  // [0] long segments, [32] middle ones
+    int* nmid = longs + 32;
+    int* big = longs + 128;
     int* mid = big + ncells;
-    cudaError_t e = cudaMemsetAsync(cnt, 0, (size_t)(ncells + 1) * sizeof(uint32_t), s);
+    cudaError_t e = cudaMemsetAsync(longs, 0, 128 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(cnt, 0, (size_t)(ncells + 1) * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     if (np > 0) k_count_dst<<<grid, 256, 0, s>>>(pairs, np, cnt, body_count, interactions);
-    e = cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, cnt, off, ncells + 1, s);
+    size_t bytes = tmp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(tmp, bytes, cnt, off, ncells + 1, s);
     if (e != cudaSuccess || np == 0) return e;
     k_scatter_dst<<<grid, 256, 0, s>>>(pairs, np, off, cnt, src_unsorted);
-    e = cudaMemsetAsync(nbig, 0, 128 * sizeof(int), s);
-    if (e != cudaSuccess) return e;
     k_sort_segments<<<grid_for((size_t)ncells * 32, 256, 148u * 64u), 256, 0, s>>>(off, ncells, src_unsorted, src,
                                                                                    mid, nmid, big, nbig);
     k_sort_segments_large<128, SEG_MID><<<148 * 12, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src, mid,
                                                                                           nmid);
-    k_sort_segments_large<256, 0><<<148 * 8, 256, 0, s>>>(off, src_unsorted, src, big, nbig);
     return cudaGetLastError();
+}
+
+// bounds of the long segments listed in `big`
+__global__ void k_long_bounds(const uint32_t* __restrict__ off, const int* __restrict__ big, int nbig,
+                              uint32_t* __restrict__ b, uint32_t* __restrict__ e) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x) {
+        const int c = big[i];
+        b[i] = off[c];
+        e[i] = off[c + 1];
+    }
+}
+
+size_t long_segments_temp(int nitems, int nlong, int end_bit) {
+    size_t bytes = 0;
+    cub::DeviceSegmentedRadixSort::SortKeys(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, nitems,
+                                            nlong, (const uint32_t*)nullptr, (const uint32_t*)nullptr, 0, end_bit);
+    return bytes;
+}
+
+cudaError_t sort_long_segments(void* tmp, size_t tmp_bytes, const uint32_t* off, const int* longs, int nlong,
+                               const uint32_t* src_unsorted, uint32_t* src, int nitems, int end_bit, uint32_t* bounds,
+                               cudaStream_t s) {
+    if (nlong == 0) return cudaSuccess;
+    k_long_bounds<<<grid_for(nlong, 256), 256, 0, s>>>(off, longs + 128, nlong, bounds, bounds + nlong);
+    size_t bytes = tmp_bytes;
+    return cub::DeviceSegmentedRadixSort::SortKeys(tmp, bytes, src_unsorted, src, nitems, nlong, bounds,
+                                                   bounds + nlong, 0, end_bit, s);
 }
 
 }  // namespace fmmx

@@ -634,15 +634,23 @@ void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const
     k_p2p_plan<<<grid, 256, 0, s>>>(ncells, L, count, units, scratch);
 }
 
-void launch_p2p_mixed(int tile, unsigned grid, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
+template <int TILE>
+static void launch_tile(int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, const double* x,
+                        const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
+                        double* az, double* pot) {
+    int per_sm = 0;  // persistent blocks: as many as fit on an SM at once
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2p_mixed<TILE>, P2PM_BLOCK, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    k_p2p_mixed<TILE><<<nsm * per_sm, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+}
+
+void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
                       const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
                       double* ay, double* az, double* pot) {
-    if (tile <= 128)
-        k_p2p_mixed<128><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
-    else if (tile <= 256)
-        k_p2p_mixed<256><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
-    else
-        k_p2p_mixed<512><<<grid, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+    if (tile <= 128) launch_tile<128>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+    else if (tile <= 256) launch_tile<256>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+    else launch_tile<512>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
     k_p2p_combine<<<grid_for((size_t)ncells * 32, 256), 256, 0, s>>>(ncells, cv, U, ax, ay, az, pot);
 }
 

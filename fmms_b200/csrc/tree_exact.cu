@@ -716,15 +716,23 @@ __global__ void k_fprepass(CellsView cells, const double* __restrict__ x, const 
     }
 }
 
+// cx, cy, cz, rho of every cell in one 32-byte record, for the walk
+__global__ void k_pack_geo(int nc, const double* __restrict__ cx, const double* __restrict__ cy,
+                           const double* __restrict__ cz, const double* __restrict__ rho, double4* __restrict__ geo) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        geo[c] = make_double4(cx[c], cy[c], cz[c], rho[c]);
+}
+
 // ------------------------------------------------------------ MAC
 // error_estimate + accept, mac.rs:23-95 (operation order kept, including the
 // inner r*r of error_estimate).
 __device__ __forceinline__ bool accept_dehnen(const CellsView& cv, const MacParams& mp, const double* __restrict__ pows,
-                                              const double* __restrict__ fminv, int a, int b) {
-    const double ax = cv.cx[a], ay = cv.cy[a], az = cv.cz[a];
-    const double dx = cv.cx[b] - ax, dy = cv.cy[b] - ay, dz = cv.cz[b] - az;
+                                              const double* __restrict__ fminv, int a, int b, const double4 ga,
+                                              const double4 gb) {
+    const double ax = ga.x, ay = ga.y, az = ga.z;
+    const double dx = gb.x - ax, dy = gb.y - ay, dz = gb.z - az;
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const double ra = cv.rho[a], rb = cv.rho[b];
+    const double ra = ga.w, rb = gb.w;
     const double sum_rho = ra + rb;
     if (r2 <= sum_rho * sum_rho) return false;
     const double r = sqrt(r2);
@@ -752,11 +760,11 @@ __device__ __forceinline__ bool accept_dehnen(const CellsView& cv, const MacPara
 
 // Separation condition (extension, with softening): the bodies of the two
 // cells are at least mp.gap apart, r - rho_A - rho_B >= gap.
-__device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp, int a, int b) {
+__device__ __forceinline__ bool gap_ok(const MacParams& mp, const double4 ga, const double4 gb) {
     if (!(mp.gap > 0.0)) return true;
-    const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
+    const double dx = gb.x - ga.x, dy = gb.y - ga.y, dz = gb.z - ga.z;
     const double r2 = dx * dx + dy * dy + dz * dz;
-    return sqrt(r2) - (cv.rho[a] + cv.rho[b]) >= mp.gap;
+    return sqrt(r2) - (ga.w + gb.w) >= mp.gap;
 }
 
 // The geometric MAC (extension): accept when (rho_A + rho_B) < theta r, both
@@ -765,10 +773,10 @@ __device__ __forceinline__ bool gap_ok(const CellsView& cv, const MacParams& mp,
 // two directions and gap_ok evaluate the same r2 (the squares of b - a and
 // a - b are equal bit for bit) and the same rho sum (addition commutes), so
 // one square root decides all three.
-__device__ __forceinline__ bool accept_theta_pair(const CellsView& cv, const MacParams& mp, int a, int b) {
-    const double dx = cv.cx[b] - cv.cx[a], dy = cv.cy[b] - cv.cy[a], dz = cv.cz[b] - cv.cz[a];
+__device__ __forceinline__ bool accept_theta_pair(const MacParams& mp, const double4 ga, const double4 gb) {
+    const double dx = gb.x - ga.x, dy = gb.y - ga.y, dz = gb.z - ga.z;
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const double sum_rho = cv.rho[a] + cv.rho[b];
+    const double sum_rho = ga.w + gb.w;
     const double r = sqrt(r2);
     if (!(sum_rho < mp.theta * r)) return false;
     return !(mp.gap > 0.0) || r - sum_rho >= mp.gap;
@@ -782,6 +790,22 @@ __device__ __forceinline__ bool accept_theta_pair(const CellsView& cv, const Mac
 // lists, a prefix sum of the child-pair counts for the next frontier); the
 // order within a list is arbitrary, the directed lists are sorted afterwards.
 enum { WK_NONE = 0, WK_M2L = 1, WK_P2P = 2, WK_SPLIT_SELF = 3, WK_SPLIT = 4 };
+
+// children of a cell: 8 ids (-1 absent), 32-byte aligned, read as two int4
+__device__ __forceinline__ void load_children(const CellsView& cv, int c, int (&ch)[8]) {
+    const int4* p = reinterpret_cast<const int4*>(cv.child + 8 * (size_t)c);
+    const int4 u = p[0], v = p[1];
+    ch[0] = u.x; ch[1] = u.y; ch[2] = u.z; ch[3] = u.w;
+    ch[4] = v.x; ch[5] = v.y; ch[6] = v.z; ch[7] = v.w;
+}
+__device__ __forceinline__ int n_children(const CellsView& cv, int c) {
+    int ch[8];
+    load_children(cv, c, ch);
+    int n = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) n += ch[o] >= 0;
+    return n;
+}
 
 __device__ __forceinline__ int warp_append(int* counter, bool mine, int lane) {
     const unsigned mask = __ballot_sync(0xffffffffu, mine);
@@ -821,17 +845,17 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
                 } else {
                     kind = WK_SPLIT_SELF;
                     sc = a;
-                    int nc = 0;
-                    for (int o = 0; o < 8; ++o) nc += cv.child[8 * a + o] >= 0;
+                    const int nc = n_children(cv, a);
                     npush = nc * (nc + 1) / 2;
                 }
             } else {
+                const double4 ga = cv.geo[a], gb = cv.geo[b];
                 bool acc;
                 if (mp.mode == FMMX_MAC_DEHNEN)
-                    acc = accept_dehnen(cv, mp, pows, fminv, a, b) && accept_dehnen(cv, mp, pows, fminv, b, a) &&
-                          gap_ok(cv, mp, a, b);
+                    acc = accept_dehnen(cv, mp, pows, fminv, a, b, ga, gb) &&
+                          accept_dehnen(cv, mp, pows, fminv, b, a, gb, ga) && gap_ok(mp, ga, gb);
                 else
-                    acc = accept_theta_pair(cv, mp, a, b);
+                    acc = accept_theta_pair(mp, ga, gb);
                 if (acc) {
                     kind = WK_M2L;
                 } else if (la && lb) {
@@ -839,9 +863,9 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
                 } else {
                     // split b when a is a leaf or b is the larger cell, else split a
                     kind = WK_SPLIT;
-                    split_a = lb || (!la && cv.rho[a] >= cv.rho[b]);
+                    split_a = lb || (!la && ga.w >= gb.w);
                     sc = split_a ? a : b;
-                    for (int o = 0; o < 8; ++o) npush += cv.child[8 * sc + o] >= 0;
+                    npush = n_children(cv, sc);
                 }
             }
         }
@@ -871,14 +895,18 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
             continue;
         }
         int pos = base + incl - npush;
-        const int32_t* ch = cv.child + 8 * sc;
+        int ch[8];
+        if (npush) load_children(cv, sc, ch);
         if (kind == WK_SPLIT_SELF) {
+#pragma unroll
             for (int i = 0; i < 8; ++i) {
                 if (ch[i] < 0) continue;
+#pragma unroll
                 for (int j = i; j < 8; ++j)
                     if (ch[j] >= 0) fout[pos++] = make_uint2(ch[i], ch[j]);
             }
         } else if (kind == WK_SPLIT) {
+#pragma unroll
             for (int o = 0; o < 8; ++o) {
                 if (ch[o] < 0) continue;
                 fout[pos++] = split_a ? make_uint2(ch[o], b) : make_uint2(a, ch[o]);
