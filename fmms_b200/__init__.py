@@ -70,6 +70,7 @@ class Config(C.Structure):
         ("soft_gap", C.c_double),
         ("use_graphs", C.c_int),
         ("overlap", C.c_int),
+        ("device_budget_bytes", C.c_uint64),
     ]
 
 
@@ -94,6 +95,8 @@ class Stats(C.Structure):
         ("ms_l2p", C.c_double),
         ("ms_evaluate", C.c_double),
         ("kernel_launches", C.c_uint64),
+        ("walk_retries", C.c_uint64),
+        ("device_bytes", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -184,14 +187,16 @@ class Fmm:
     keyword arguments select the extensions: ``mac='theta'`` with ``theta``,
     ``softening``, ``precision='mixed'``, ``center='sphere'`` (as
     ``Fmm::with_center``), ``m2l='naive'|'rotation'``, ``soft_gap`` (M2L only
-    between cells whose bodies are soft_gap * softening apart).
+    between cells whose bodies are soft_gap * softening apart),
+    ``device_budget_bytes`` (device memory the context may hold; beyond it a
+    call raises FmmError with status "over budget").
     """
 
     def __init__(self, mass, pos, p: int = 8, eps: float = 1e-5, n_leaf: int = 16, *, mac: str = "dehnen",
                  theta: float = 0.5, softening: float = 0.0, precision: str = "plain", center: str = "com",
                  m2l: str = "auto", device: int = 0, stream: int | None = None, p2p_tile: int = 0,
                  preemptible: bool = False, soft_gap: float = 0.0, use_graphs: bool = True,
-                 overlap: bool = True):
+                 overlap: bool = True, device_budget_bytes: int = 0):
         cfg = Config()
         lib().fmmx_config_default(C.byref(cfg))
         cfg.p = int(p)
@@ -210,6 +215,7 @@ class Fmm:
         cfg.soft_gap = float(soft_gap)
         cfg.use_graphs = 1 if use_graphs else 0
         cfg.overlap = 1 if overlap else 0
+        cfg.device_budget_bytes = int(device_budget_bytes)
         self.cfg = cfg
         self.p = cfg.p
         h = _vp()

@@ -93,7 +93,14 @@ struct CellsView {
     const double4* geo;  // cx, cy, cz, rho of each cell in one 32-byte record (the walk's loads)
 };
 
-static inline unsigned grid_for(size_t n, int block, unsigned cap = 148u * 32u) {
+// SM count of the device, read when a context is created (grid sizes of the
+// grid-stride and persistent kernels are multiples of it)
+inline int g_nsm = 148;
+
+// blocks for n items at `block` threads, at most cap (default 32 per SM; the
+// kernels stride over the rest)
+static inline unsigned grid_for(size_t n, int block, unsigned cap = 0) {
+    if (cap == 0) cap = 32u * (unsigned)g_nsm;
     size_t g = (n + block - 1) / block;
     if (g < 1) g = 1;
     if (g > cap) g = cap;

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -27,15 +28,34 @@ using namespace fmmx;
 
 namespace {
 
+// Device-memory budget of a context (fmmx_config.device_budget_bytes): every
+// engine buffer is charged to it, and the allocation that would take the
+// context above it fails with FMMX_OVER_BUDGET, naming the buffer, the bytes
+// it needs and the limit (the reference's GPU OverBudget error,
+// crates/visual/src/gpufmm.rs:1653-1672, after which its callers fall back).
+struct Budget {
+    uint64_t limit = 0;  // bytes; 0: no limit
+    uint64_t used = 0;
+    bool over = false;   // the last refusal, until reported
+    uint64_t asked = 0;
+};
+// the budget of the context whose API call runs on this thread
+thread_local Budget* tl_budget = nullptr;
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t cap = 0;
+    Budget* bud = nullptr;  // charged for this buffer
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            if (bud) bud->used -= cap * sizeof(T);
+        }
         p = nullptr;
         cap = 0;
+        bud = nullptr;
     }
     // Grows by at least half of the current capacity, so a context that sees
     // slowly growing inputs (a serving loop's forests) reallocates -- and
@@ -47,8 +67,18 @@ struct DBuf {
     cudaError_t ensure(size_t n) {
         if (n <= cap && p) return cudaSuccess;
         const size_t grown = cap + cap / 2;
-        release();
         size_t want = std::max<size_t>(std::max<size_t>(n + n / 8, grown), 1);
+        Budget* b = tl_budget;
+        if (b && b->limit) {
+            const uint64_t base = b->used - (p && bud == b ? cap * sizeof(T) : 0);
+            if (base + want * sizeof(T) > b->limit) want = std::max<size_t>(n, 1);  // no slack
+            if (base + want * sizeof(T) > b->limit) {
+                b->over = true;
+                b->asked = want * sizeof(T);
+                return cudaErrorMemoryAllocation;
+            }
+        }
+        release();
         cudaError_t e = cudaMalloc((void**)&p, want * sizeof(T));
         if (e != cudaSuccess && want > n) {  // no room for the slack: exactly n
             cudaGetLastError();
@@ -61,8 +91,17 @@ struct DBuf {
             return e;
         }
         cap = want;
+        bud = b;
+        if (bud) bud->used += cap * sizeof(T);
         return cudaSuccess;
     }
+};
+
+// charges the allocations of one API call to its context's budget
+struct BudgetScope {
+    Budget* prev;
+    explicit BudgetScope(Budget* b) : prev(tl_budget) { tl_budget = b; }
+    ~BudgetScope() { tl_budget = prev; }
 };
 
 int rot_moff_host(int k) { return 4 * (k * (k + 1) * (2 * k + 1) / 6); }
@@ -81,6 +120,7 @@ struct Status {
 }  // namespace
 
 struct fmmx_ctx {
+    Budget budget;  // first: outlives every buffer charged to it
     fmmx_config cfg;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -154,6 +194,8 @@ struct fmmx_ctx {
     DBuf<int> wcounts;
     DBuf<unsigned long long> wpops, inter;
     uint32_t cap_front = 0, cap_m2l = 0, cap_p2p = 0;
+    uint64_t walk_cap0 = 0;  // FMMX_TEST_WALK_CAPACITY (tests of the overflow retry); 0: sized by the tree
+    int walk_retries = 0;
 
     // directed lists
     // per destination cell c: sources src[off[c] .. off[c+1]), ascending
@@ -187,6 +229,13 @@ fmmx_status fail(fmmx_ctx* c, fmmx_status s, const std::string& msg) {
 }
 
 fmmx_status cuda_fail(fmmx_ctx* c, cudaError_t e, const char* where) {
+    if (e == cudaErrorMemoryAllocation && c->budget.over) {
+        c->budget.over = false;
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s needs %.1f MiB, device budget %.1f MiB (%.1f MiB in use)", where,
+                      c->budget.asked / 1048576.0, c->budget.limit / 1048576.0, c->budget.used / 1048576.0);
+        return fail(c, FMMX_OVER_BUDGET, buf);
+    }
     std::string m = std::string(where) + ": " + cudaGetErrorString(e);
     cudaGetLastError();
     if (e == cudaErrorMemoryAllocation) return fail(c, FMMX_OUT_OF_MEMORY, m);
@@ -353,7 +402,6 @@ M2lChoice m2l_choice(const fmmx_config& c) {
     return c.p <= kRotwMaxP ? M2L_ROT_WARP : M2L_ROT_BLOCK;
 }
 
-const unsigned kGrid = 148u * 8u;
 
 // ---------------------------------------------------------------- build
 // nsys > 1 builds a forest: system s is inputs [off[s], off[s+1]) (host
@@ -444,7 +492,7 @@ fmmx_status build_impl(fmmx_ctx* ctx, size_t n, const double* d_pos, const doubl
         if (nsys == 1) k_tree_init<<<1, 32, 0, s>>>(tn, (uint32_t)n, ctx->lvl.p);
         else k_tree_init_forest<<<grid_for(nsys, 128), 128, 0, s>>>(tn, ctx->sys_off.p, nsys, ctx->lvl.p);
         LCOUNT(1 + FMMX_NLEVELS);
-        const unsigned gl = std::min<unsigned>(grid_for(cap, 256), kGrid);
+        const unsigned gl = std::min<unsigned>(grid_for(cap, 256), 8u * (unsigned)ctx->nsm);
         for (int L = 0; L < FMMX_NLEVELS; ++L)
             k_build_level<<<gl, 256, 0, s>>>(tn, ctx->keys_sorted.p, L, (long long)ctx->cfg.n_leaf, cap, ctx->lvl.p,
                                               ctx->flags.p);
@@ -538,9 +586,16 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
     // capacities follow the current tree (a context may see trees of very
     // different sizes, e.g. the forests of a serving loop) and grow on overflow
     auto at_least = [](uint32_t c, uint64_t w) { return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(c, w), 0x7fffffffull); };
-    ctx->cap_front = at_least(ctx->cap_front, 64ull * nc + 1024);
-    ctx->cap_m2l = at_least(ctx->cap_m2l, 64ull * nc + 1024);
-    ctx->cap_p2p = at_least(ctx->cap_p2p, 32ull * nc + 1024);
+    if (ctx->walk_cap0 > 0) {  // test knob: start from the given capacity (and grow on overflow)
+        ctx->cap_front = at_least(ctx->cap_front, ctx->walk_cap0);
+        ctx->cap_m2l = at_least(ctx->cap_m2l, ctx->walk_cap0);
+        ctx->cap_p2p = at_least(ctx->cap_p2p, ctx->walk_cap0);
+    } else {
+        ctx->cap_front = at_least(ctx->cap_front, 64ull * nc + 1024);
+        ctx->cap_m2l = at_least(ctx->cap_m2l, 64ull * nc + 1024);
+        ctx->cap_p2p = at_least(ctx->cap_p2p, 32ull * nc + 1024);
+    }
+    ctx->walk_retries = 0;
     CK(ctx->wcounts.ensure(WC_SIZE), "alloc");
     CK(ctx->wpops.ensure(1), "alloc");
     MacParams mp;
@@ -578,7 +633,7 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
         const int max_iter = 8 * FMMX_NLEVELS + 16;
         for (int it = 0; it < max_iter && !done;) {
             for (int b = 0; b < 6; ++b, ++it) {
-                k_walk_iter<<<kGrid, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
+                k_walk_iter<<<8u * (unsigned)ctx->nsm, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
                 LCOUNT(1);
                 CK(cudaMemsetAsync(ctx->wcounts.p + cur, 0, sizeof(int), s), "memset");
                 cur ^= 1;
@@ -591,6 +646,7 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
         if (!done) return fail(ctx, FMMX_TIMEOUT, "dual walk did not terminate");
         if (hc[WC_OVERFLOW]) {
             if (attempt > 24) return fail(ctx, FMMX_OUT_OF_MEMORY, "walk capacity");
+            ctx->walk_retries++;
             auto grow = [](uint32_t c, int used) {
                 uint64_t w2 = std::max<uint64_t>(4ull * c, (uint64_t)used + (uint64_t)used / 2 + 1024);
                 return (uint32_t)std::min<uint64_t>(w2, 0x7fffffffull);
@@ -712,7 +768,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 3);  // m2l, l2l per level, p2p + combine, l2p
     for (int L = 1; L < ctx->nlevels; ++L) {
         const int cnt = ctx->lvl_count[L];
-        const unsigned g = std::min<unsigned>(cnt, 148u * 16u);
+        const unsigned g = std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm);
         launch_l2l_mixed(L <= 3, g, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->c_parent.p, ctx->ell.p,
                          p, ctx->loc_f.p);
     }
@@ -783,7 +839,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         // normalised FP32 upward pass; FP64 accumulation on the top three levels
         for (int L = ctx->nlevels - 1; L >= 0; --L) {
             const int cnt = ctx->lvl_count[L];
-            const unsigned g = std::min<unsigned>(cnt, 148u * 16u);
+            const unsigned g = std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm);
             launch_upward_mixed(L <= 2, g, 4, s, ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->ell.p,
                                 ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->mom_f.p);
         }
@@ -795,7 +851,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
             CK(cudaFuncSetAttribute(k_upward_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
         for (int L = ctx->nlevels - 1; L >= 0; --L) {
             const int cnt = ctx->lvl_count[L];
-            unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, kGrid);
+            unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, 8u * (unsigned)ctx->nsm);
             k_upward_exact<<<g, 32 * warps, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->x.p,
                                                        ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->moments.p, ctx->pows.p,
                                                        dehnen ? ctx->f.p : nullptr, ctx->fmin.p);
@@ -855,7 +911,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     if (tm) CK(cudaEventRecord(ev[11], s), "event");  // far field from here
     CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
     if (ctx->n_m2l > 0) {
-        const unsigned g = std::min<unsigned>(nc, 148u * 16u);
+        const unsigned g = std::min<unsigned>(nc, 16u * (unsigned)ctx->nsm);
         const M2lChoice ch = m2l_choice(ctx->cfg);
         if (ch == M2L_ROT_WARP) {
             int* work = nullptr;  // preemptible: one block per destination cell
@@ -881,7 +937,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         const size_t smem = 2 * (size_t)dim * sizeof(zd);
         for (int L = 1; L < ctx->nlevels; ++L) {
             const int cnt = ctx->lvl_count[L];
-            k_l2l_f64<<<std::min<unsigned>(cnt, 148u * 16u), 128, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L],
+            k_l2l_f64<<<std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm), 128, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L],
                                                                             cnt, cv, ctx->c_parent.p, p,
                                                                             ctx->locals.p);
         }
@@ -942,6 +998,7 @@ void fmmx_config_default(fmmx_config* c) {
     c->soft_gap = 0.0;
     c->use_graphs = 1;
     c->overlap = 1;
+    c->device_budget_bytes = 0;
 }
 
 const char* fmmx_status_string(fmmx_status s) {
@@ -986,6 +1043,9 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (cudaSetDevice(c.device) != cudaSuccess) return FMMX_DEVICE_ERROR;
     fmmx_ctx* ctx = new fmmx_ctx();
     ctx->cfg = c;
+    ctx->budget.limit = c.device_budget_bytes;
+    BudgetScope bscope(&ctx->budget);
+    if (const char* wc = std::getenv("FMMX_TEST_WALK_CAPACITY")) ctx->walk_cap0 = std::strtoull(wc, nullptr, 10);
     std::memset(&ctx->st, 0, sizeof(ctx->st));
     if (c.stream) {
         ctx->stream = (cudaStream_t)c.stream;
@@ -1014,6 +1074,8 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
             }
     }
     cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
+    if (ctx->nsm < 1) ctx->nsm = 1;
+    g_nsm = ctx->nsm;
     make_tables(ctx->tab);
     {
         RotwTables rt;
@@ -1061,6 +1123,7 @@ const char* fmmx_last_error(const fmmx_ctx* ctx) { return ctx ? ctx->err.c_str()
 
 fmmx_status fmmx_build_device(fmmx_ctx* ctx, size_t n, const double* d_pos, const double* d_mass) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!d_pos || !d_mass) return fail(ctx, FMMX_INVALID_ARG, "null input");
     cudaSetDevice(ctx->cfg.device);
     return build_impl(ctx, n, d_pos, d_mass);
@@ -1068,6 +1131,7 @@ fmmx_status fmmx_build_device(fmmx_ctx* ctx, size_t n, const double* d_pos, cons
 
 fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double* mass) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!pos || !mass) return fail(ctx, FMMX_INVALID_ARG, "null input");
     if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input (the reference asserts !parts.is_empty(), tree.rs:95)");
     cudaSetDevice(ctx->cfg.device);
@@ -1083,6 +1147,7 @@ fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double*
 fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* d_pos,
                                        const double* d_mass) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!d_pos || !d_mass || !offsets || nsys == 0 || nsys > (1u << 24)) return fail(ctx, FMMX_INVALID_ARG, "bad input");
     cudaSetDevice(ctx->cfg.device);
     return build_impl(ctx, (size_t)offsets[nsys], d_pos, d_mass, (int)nsys, offsets);
@@ -1091,6 +1156,7 @@ fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_
 fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* pos,
                                 const double* mass) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!pos || !mass || !offsets || nsys == 0 || nsys > (1u << 24)) return fail(ctx, FMMX_INVALID_ARG, "bad input");
     const size_t n = (size_t)offsets[nsys];
     if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input");
@@ -1107,6 +1173,7 @@ fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offs
 fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc,
                                  double* d_pot) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!d_acc) return fail(ctx, FMMX_INVALID_ARG, "null output");
     cudaSetDevice(ctx->cfg.device);
     if (!d_pot) {
@@ -1121,6 +1188,7 @@ static constexpr int kGraphMinUses = 2;
 fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, const double* d_mass, double* d_acc,
                                  double* d_pot, double dt, int nsteps, int scheme, int refresh_every) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!d_pos || !d_vel || !d_mass || !d_acc || nsteps < 0 || refresh_every < 1 || (scheme != 0 && scheme != 1))
         return fail(ctx, FMMX_INVALID_ARG, "bad leapfrog arguments");
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "leapfrog needs a built tree (build + evaluate first)");
@@ -1223,6 +1291,7 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, co
 
 fmmx_status fmmx_evaluate(fmmx_ctx* ctx, const double* pos, const double* mass, double* acc, double* pot) {
     if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
     if (!acc) return fail(ctx, FMMX_INVALID_ARG, "null output");
     if (!ctx->built) return fail(ctx, FMMX_NOT_BUILT, "evaluate before build");
     cudaSetDevice(ctx->cfg.device);
@@ -1276,6 +1345,8 @@ fmmx_status fmmx_get_stats(const fmmx_ctx* ctx, fmmx_stats* out) {
     out->p2p_interactions = ctx->p2p_inter;
     out->m2l_directed = 2ull * (uint64_t)ctx->n_m2l;
     out->kernel_launches = ctx->launches;
+    out->walk_retries = (uint64_t)ctx->walk_retries;
+    out->device_bytes = ctx->budget.used;
     return FMMX_OK;
 }
 

@@ -289,9 +289,9 @@ cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs,
     e = cub::DeviceScan::ExclusiveSum(tmp, bytes, cnt, off, ncells + 1, s);
     if (e != cudaSuccess || np == 0) return e;
     k_scatter_dst<<<grid, 256, 0, s>>>(pairs, np, off, cnt, src_unsorted);
-    k_sort_segments<<<grid_for((size_t)ncells * 32, 256, 148u * 64u), 256, 0, s>>>(off, ncells, src_unsorted, src,
+    k_sort_segments<<<grid_for((size_t)ncells * 32, 256, 64u * g_nsm), 256, 0, s>>>(off, ncells, src_unsorted, src,
                                                                                    mid, nmid, big, nbig);
-    k_sort_segments_large<128, SEG_MID><<<148 * 12, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src, mid,
+    k_sort_segments_large<128, SEG_MID><<<12 * g_nsm, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src, mid,
                                                                                           nmid);
     return cudaGetLastError();
 }

@@ -26,6 +26,13 @@
 extern "C" {
 #endif
 
+/* Status codes. FMMX_OVER_BUDGET is the reference GPU backend's OverBudget
+ * (crates/visual/src/gpufmm.rs:1653-1672): an engine buffer would take the
+ * context above its device_budget_bytes; the message names the buffer, the
+ * bytes and the limit, and the context stays usable (the caller can retry
+ * smaller or fall back). FMMX_LEAF_OVERFLOW mirrors the reference's
+ * OverfullLeaf (gpufmm.rs:1377-1379, a leaf above its 64-lane kernels); no
+ * kernel here bounds the bodies of a leaf, so it is never returned. */
 typedef enum fmmx_status {
     FMMX_OK = 0,
     FMMX_INVALID_ARG = 1,
@@ -84,6 +91,8 @@ typedef struct fmmx_config {
     int overlap;       /* 1 (default): an evaluation runs on two streams (walk and lists beside the upward pass,
                           P2P beside M2L and L2L; the per-stage times then overlap); 0: one stream, every
                           stage alone on the device (for timing single kernels) */
+    uint64_t device_budget_bytes; /* device memory the context may hold, in bytes (0, the default: no limit);
+                          an allocation above it fails with FMMX_OVER_BUDGET */
 } fmmx_config;
 
 typedef struct fmmx_stats {
@@ -106,6 +115,8 @@ typedef struct fmmx_stats {
     double ms_l2p;
     double ms_evaluate;        /* whole evaluate, device time */
     uint64_t kernel_launches;  /* engine kernels launched by the last build + evaluate */
+    uint64_t walk_retries;     /* walks of the last evaluate redone with larger buffers after an overflow */
+    uint64_t device_bytes;     /* device memory held by the context */
 } fmmx_stats;
 
 typedef struct fmmx_ctx fmmx_ctx;

@@ -84,3 +84,16 @@ def test_noalloc_limit_matches_header():
     txt = open(os.path.join(ROOT, "include", "fmmx.h")).read()
     m = re.search(r"#define\s+FMMX_DIRECT_NOALLOC_MAX_TARGETS\s+(\d+)", txt)
     assert m and int(m.group(1)) == fx.DIRECT_NOALLOC_MAX_TARGETS
+
+
+def test_config_and_stats_layout_match_header():
+    """The ctypes structures hold every field of fmmx_config and fmmx_stats,
+    in the header's order (new fields appended at the end)."""
+    import fmms_b200 as fx
+
+    txt = open(os.path.join(ROOT, "include", "fmmx.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    for name, cls in (("fmmx_config", fx.Config), ("fmmx_stats", fx.Stats)):
+        body = re.search(r"typedef struct " + name + r" \{(.*?)\} " + name + ";", txt, flags=re.S).group(1)
+        fields = re.findall(r"\b([a-z_0-9]+)\s*;", body)
+        assert fields == [f for f, _ in cls._fields_], name
