@@ -42,13 +42,26 @@ struct Budget {
 // the budget of the context whose API call runs on this thread
 thread_local Budget* tl_budget = nullptr;
 
+// Every device buffer of a context registers itself while the context is
+// constructed, so that the context can drop all of them (a cache: the next
+// call reallocates) after a call fails over its budget.
+struct DBufBase {
+    DBufBase();
+    virtual ~DBufBase() = default;
+    virtual void release() = 0;
+};
+thread_local std::vector<DBufBase*>* tl_registry = nullptr;
+DBufBase::DBufBase() {
+    if (tl_registry) tl_registry->push_back(this);
+}
+
 template <class T>
-struct DBuf {
+struct DBuf : DBufBase {
     T* p = nullptr;
     size_t cap = 0;
     Budget* bud = nullptr;  // charged for this buffer
-    ~DBuf() { release(); }
-    void release() {
+    ~DBuf() override { release(); }
+    void release() override {
         if (p) {
             cudaFree(p);
             if (bud) bud->used -= cap * sizeof(T);
@@ -149,6 +162,7 @@ struct fmmx_ctx {
         if (step_graph) cudaGraphExecDestroy(step_graph);
         step_graph = nullptr;
     }
+    std::vector<DBufBase*> cache;  // every buffer but the constant tables
     int n_m2l = 0, n_p2p = 0;
     unsigned long long pops = 0, p2p_inter = 0;
 
@@ -240,6 +254,22 @@ fmmx_status cuda_fail(fmmx_ctx* c, cudaError_t e, const char* where) {
     cudaGetLastError();
     if (e == cudaErrorMemoryAllocation) return fail(c, FMMX_OUT_OF_MEMORY, m);
     return fail(c, FMMX_DEVICE_ERROR, m);
+}
+
+// A call that failed over the budget leaves the context with whatever its
+// buffers had grown to: drop them all (the next call reallocates what it
+// needs), so that a smaller system fits again.
+fmmx_status finish(fmmx_ctx* ctx, fmmx_status st) {
+    if (st != FMMX_OVER_BUDGET) return st;
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
+    cudaGetLastError();
+    ctx->drop_graph();
+    for (DBufBase* b : ctx->cache) b->release();
+    ctx->built = ctx->evaluated = ctx->lists_valid = false;
+    ctx->cap_front = ctx->cap_m2l = ctx->cap_p2p = 0;
+    ctx->tcap = 0;
+    return st;
 }
 
 #define CK(expr, where)                                   \
@@ -845,16 +875,28 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         }
         CKL("upward (mixed)");
     } else {
-        const int warps = 4;
-        const size_t smem = (size_t)warps * 2 * dim * sizeof(zd);
+        const int warps = 2;  // the P2M tables take 35 KB of shared memory per warp at p = 10
+        const size_t smem = (size_t)warps * upward_exact_smem_per_warp(p);
         if (smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_upward_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+        const size_t smem_b = 16 * (size_t)dim * sizeof(zd);
+        if (smem_b > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_m2m_exact_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b),
+               "attr");
+        // per level: the leaves' P2M (a warp per leaf), then the internal
+        // cells' M2M (a block per cell)
         for (int L = ctx->nlevels - 1; L >= 0; --L) {
             const int cnt = ctx->lvl_count[L];
-            unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, 8u * (unsigned)ctx->nsm);
+            unsigned g = std::min<unsigned>((cnt + warps - 1) / warps, 16u * (unsigned)ctx->nsm);
             k_upward_exact<<<g, 32 * warps, smem, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, ctx->x.p,
                                                        ctx->y.p, ctx->z.p, ctx->m.p, p, ctx->moments.p, ctx->pows.p,
-                                                       dehnen ? ctx->f.p : nullptr, ctx->fmin.p);
+                                                       dehnen ? ctx->f.p : nullptr, ctx->fmin.p, 1);
+            if (L < ctx->nlevels - 1) {
+                k_m2m_exact_block<<<std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm), 256, smem_b, s>>>(
+                    ctx->level_cells.p, ctx->lvl_start[L], cnt, cv, p, ctx->moments.p, ctx->pows.p,
+                    dehnen ? ctx->f.p : nullptr, ctx->fmin.p);
+                LCOUNT(1);
+            }
         }
         CKL("upward");
         if (mixed) {  // the MAC saw exact FP64 moments; the translations use FP32
@@ -1041,7 +1083,12 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     }
     if (c.device < 0 || c.device >= ndev) return FMMX_INVALID_ARG;
     if (cudaSetDevice(c.device) != cudaSuccess) return FMMX_DEVICE_ERROR;
+    std::vector<DBufBase*> reg;
+    tl_registry = &reg;
     fmmx_ctx* ctx = new fmmx_ctx();
+    tl_registry = nullptr;
+    for (DBufBase* b : reg)
+        if (b != &ctx->swap_dev) ctx->cache.push_back(b);
     ctx->cfg = c;
     ctx->budget.limit = c.device_budget_bytes;
     BudgetScope bscope(&ctx->budget);
@@ -1126,7 +1173,7 @@ fmmx_status fmmx_build_device(fmmx_ctx* ctx, size_t n, const double* d_pos, cons
     BudgetScope bscope(&ctx->budget);
     if (!d_pos || !d_mass) return fail(ctx, FMMX_INVALID_ARG, "null input");
     cudaSetDevice(ctx->cfg.device);
-    return build_impl(ctx, n, d_pos, d_mass);
+    return finish(ctx, build_impl(ctx, n, d_pos, d_mass));
 }
 
 fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double* mass) {
@@ -1141,7 +1188,7 @@ fmmx_status fmmx_build(fmmx_ctx* ctx, size_t n, const double* pos, const double*
     if (cudaMemcpyAsync(ctx->pos_in.p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(ctx->mass_in.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
-    return build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p);
+    return finish(ctx, build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p));
 }
 
 fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* d_pos,
@@ -1150,7 +1197,7 @@ fmmx_status fmmx_build_ensemble_device(fmmx_ctx* ctx, size_t nsys, const uint64_
     BudgetScope bscope(&ctx->budget);
     if (!d_pos || !d_mass || !offsets || nsys == 0 || nsys > (1u << 24)) return fail(ctx, FMMX_INVALID_ARG, "bad input");
     cudaSetDevice(ctx->cfg.device);
-    return build_impl(ctx, (size_t)offsets[nsys], d_pos, d_mass, (int)nsys, offsets);
+    return finish(ctx, build_impl(ctx, (size_t)offsets[nsys], d_pos, d_mass, (int)nsys, offsets));
 }
 
 fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offsets, const double* pos,
@@ -1167,7 +1214,7 @@ fmmx_status fmmx_build_ensemble(fmmx_ctx* ctx, size_t nsys, const uint64_t* offs
     if (cudaMemcpyAsync(ctx->pos_in.p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(ctx->mass_in.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return cuda_fail(ctx, cudaGetLastError(), "copy inputs");
-    return build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p, (int)nsys, offsets);
+    return finish(ctx, build_impl(ctx, n, ctx->pos_in.p, ctx->mass_in.p, (int)nsys, offsets));
 }
 
 fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const double* d_mass, double* d_acc,
@@ -1180,7 +1227,7 @@ fmmx_status fmmx_evaluate_device(fmmx_ctx* ctx, const double* d_pos, const doubl
         if (ctx->pot_out.ensure(ctx->n) != cudaSuccess) return fail(ctx, FMMX_OUT_OF_MEMORY, "pot buffer");
         d_pot = ctx->pot_out.p;
     }
-    return evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot);
+    return finish(ctx, evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot));
 }
 
 static constexpr int kGraphMinUses = 2;
@@ -1269,14 +1316,14 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, co
                 std::vector<uint64_t> off(ctx->sys_off_host);
                 st = build_impl(ctx, n, d_pos, d_mass, ctx->nsys, off.data());
             }
-            if (st != FMMX_OK) return st;
+            if (st != FMMX_OK) return finish(ctx, st);
             ctx->steps_since_build = 0;
             st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, false);
         } else {
             ctx->steps_since_build++;
             st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, true);
         }
-        if (st != FMMX_OK) return st;
+        if (st != FMMX_OK) return finish(ctx, st);
         if (scheme == 0) {
             k_kick<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, 0.5 * dt);
         } else {
@@ -1316,7 +1363,7 @@ fmmx_status fmmx_evaluate(fmmx_ctx* ctx, const double* pos, const double* mass, 
     if (ctx->acc_out.ensure(3 * n) != cudaSuccess || ctx->pot_out.ensure(n) != cudaSuccess)
         return fail(ctx, FMMX_OUT_OF_MEMORY, "output buffers");
     fmmx_status st = evaluate_impl(ctx, dp, dm, ctx->acc_out.p, ctx->pot_out.p);
-    if (st != FMMX_OK) return st;
+    if (st != FMMX_OK) return finish(ctx, st);
     if (cudaMemcpyAsync(acc, ctx->acc_out.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return cuda_fail(ctx, cudaGetLastError(), "copy outputs");
     if (pot && cudaMemcpyAsync(pot, ctx->pot_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)

@@ -88,9 +88,14 @@ __global__ void k_body_leaf(int nc, const uint32_t* first, const uint32_t* count
                             int32_t* body_leaf);
 __global__ void k_geometry_level(const int32_t* level_cells, int lstart, int lcnt, CellsMut cells, const double* x,
                                  const double* y, const double* z, const double* m, int center_mode);
+// bodies per round of the exact P2M (the lanes of a warp build that many Υ tables at once)
+__host__ __device__ inline int p2m_round(int p) { return p <= 12 ? 32 : (p <= 16 ? 16 : 8); }
+__host__ __device__ size_t upward_exact_smem_per_warp(int p);
 __global__ void k_upward_exact(const int32_t* level_cells, int lstart, int lcnt, CellsView cells, const double* x,
                                const double* y, const double* z, const double* m, int p, zd* moments, double* pows,
-                               const double* f, double* fmin);
+                               const double* f, double* fmin, int skip_internal);
+__global__ void k_m2m_exact_block(const int32_t* level_cells, int lstart, int lcnt, CellsView cells, int p,
+                                  zd* moments, double* pows, const double* f, double* fmin);
 __global__ void k_fprepass(CellsView cells, const double* x, const double* y, const double* z, const double* m,
                            size_t n, const uint64_t* off, int nsys, const int32_t* roots, double* f, int* err);
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);

@@ -17,13 +17,17 @@
 
 namespace fmmx {
 
-static __constant__ OrderTables c_tab;
+// The order tables in global memory: the kernels read them with lane-
+// dependent indices (a lane per order m or per degree), which the constant
+// cache would serialise over the distinct addresses; global loads are served
+// from L1 in parallel.
+static __device__ OrderTables g_tab;
 
 #define M2L_BLOCK 128
 #define M2L_OUT ((FMMX_MAXDIM + M2L_BLOCK - 1) / M2L_BLOCK)
 
 void upload_tables_m2l(const OrderTables& t, cudaStream_t s) {
-    cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
 }
 
 __device__ __forceinline__ void split_e(int e, int& n, int& m) {
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(M2L_BLOCK) k_m2l_rot_f64(DirList L, int ncells
         if (e < dim) {
             split_e(e, on[j], om[j]);
             int am = om[j] < 0 ? -om[j] : om[j];
-            fmv[j] = c_tab.fact[on[j] - am] * c_tab.fact[on[j] + am];
+            fmv[j] = g_tab.fact[on[j] - am] * g_tab.fact[on[j] + am];
         } else {
             on[j] = -1;
         }
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(M2L_BLOCK) k_m2l_rot_f64(DirList L, int ncells
                 const double rinv = rsqrt(r2);
                 double irp = rinv;
                 for (int j = 0; j < tid; ++j) irp *= rinv;
-                facr[tid] = c_tab.fact[tid] * irp;
+                facr[tid] = g_tab.fact[tid] * irp;
             }
             __syncthreads();
             // 1) back-rotate, u = in·pha·conj(M)

@@ -18,10 +18,14 @@
 
 namespace fmmx {
 
-static __constant__ OrderTables c_tab;
+// The order tables in global memory: the kernels read them with lane-
+// dependent indices (a lane per order m or per degree), which the constant
+// cache would serialise over the distinct addresses; global loads are served
+// from L1 in parallel.
+static __device__ OrderTables g_tab;
 
 void upload_tables_mixed(const OrderTables& t, cudaStream_t s) {
-    cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
 }
 
 __host__ __device__ constexpr int hx(int n, int m) { return n * (n + 1) / 2 + m; }
@@ -46,12 +50,12 @@ __device__ __forceinline__ cplx<T> half_get(const cplx<T>* v, int n, int m) {
 template <typename A>
 __device__ __forceinline__ void ups_column(A x, A y, A z, A r2, int p, int m, cplx<A>* u) {
     cplx<A> d = mk<A>(A(1), A(0));
-    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk<A>(x, y), (A)c_tab.inv2m[j]), d);
+    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk<A>(x, y), (A)g_tab.inv2m[j]), d);
     u[hx(m, m)] = d;
     cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
     for (int n = m + 1; n <= p; ++n) {
         const A a = (A)(2 * n - 1) * z;
-        cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][m]);
+        cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)g_tab.invc[n][m]);
         u[hx(n, m)] = un;
         u2 = u1;
         u1 = un;
@@ -145,13 +149,13 @@ __global__ void __launch_bounds__(UPM_BLOCK) k_upward_mixed(const int32_t* __res
                     const A mb = bod[3 * UPM_BLOCK + b];
                     const A r2 = rx * rx + ry * ry + rz * rz;
                     cplx<A> d = mk<A>(A(1), A(0));
-                    for (int q = 1; q <= mc; ++q) d = zmul(zscale(mk<A>(rx, ry), (A)c_tab.inv2m[q]), d);
+                    for (int q = 1; q <= mc; ++q) d = zmul(zscale(mk<A>(rx, ry), (A)g_tab.inv2m[q]), d);
                     cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
                     acc[hx(mc, mc)].re += d.re * mb;
                     acc[hx(mc, mc)].im += d.im * mb;
                     for (int n = mc + 1; n <= p; ++n) {
                         const A a = (A)(2 * n - 1) * rz;
-                        const cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)c_tab.invc[n][mc]);
+                        const cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)g_tab.invc[n][mc]);
                         u2 = u1;
                         u1 = un;
                         acc[hx(n, mc)].re += un.re * mb;
@@ -314,7 +318,7 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
         float p00 = 0, p11r = 0, p11i = 0, p10 = 0;
         zf d = mk<float>(1.f, 0.f);
         for (int lm = 0; lm <= p; ++lm) {
-            if (lm > 0) d = zmul(zscale(mk<float>(rx, ry), (float)c_tab.inv2m[lm]), d);
+            if (lm > 0) d = zmul(zscale(mk<float>(rx, ry), (float)g_tab.inv2m[lm]), d);
             zf u1 = d, u2 = mk<float>(0.f, 0.f);
             const float sgn = (lm & 1) ? -1.f : 1.f;
             for (int kk = lm; kk <= p; ++kk) {
@@ -323,7 +327,7 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
                     uk = d;
                 } else {
                     const float a = (float)(2 * kk - 1) * rz;
-                    uk = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (float)c_tab.invc[kk][lm]);
+                    uk = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (float)g_tab.invc[kk][lm]);
                     u2 = u1;
                     u1 = uk;
                 }

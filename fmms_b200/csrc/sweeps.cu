@@ -10,10 +10,14 @@
 
 namespace fmmx {
 
-static __constant__ OrderTables c_tab;
+// The order tables in global memory: the kernels read them with lane-
+// dependent indices (a lane per order m or per degree), which the constant
+// cache would serialise over the distinct addresses; global loads are served
+// from L1 in parallel.
+static __device__ OrderTables g_tab;
 
 void upload_tables_sweeps(const OrderTables& t, cudaStream_t s) {
-    cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
 }
 
 #define SW_BLOCK 128
@@ -30,12 +34,12 @@ __device__ __forceinline__ void split_e2(int e, int& n, int& m) {
 // Υ column m (upsilon_table_into, harmonic.rs:141-173) with negative orders.
 __device__ __forceinline__ void upsilon_column_f64(double x, double y, double z, double r2, int p, int m, zd* u) {
     zd d = mk(1.0, 0.0);
-    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk(x, y), c_tab.inv2m[j]), d);
+    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk(x, y), g_tab.inv2m[j]), d);
     u[cidx(m, m)] = d;
     zd u1 = d, u2 = mk(0.0, 0.0);
     for (int n = m + 1; n <= p; ++n) {
         const double a = (double)(2 * n - 1) * z;
-        zd un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), c_tab.invc[n][m]);
+        zd un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), g_tab.invc[n][m]);
         u[cidx(n, m)] = un;
         u2 = u1;
         u1 = un;
@@ -101,7 +105,7 @@ __global__ void k_l2p_f64(size_t n, const int32_t* __restrict__ body_leaf, const
         double p00 = 0.0, p11r = 0.0, p11i = 0.0, p10 = 0.0;
         zd d = mk(1.0, 0.0);
         for (int l = 0; l <= p; ++l) {
-            if (l > 0) d = zmul(zscale(mk(rx, ry), c_tab.inv2m[l]), d);
+            if (l > 0) d = zmul(zscale(mk(rx, ry), g_tab.inv2m[l]), d);
             zd u1 = d, u2 = mk(0.0, 0.0);
             const double sgn = (l & 1) ? -1.0 : 1.0;
             for (int kk = l; kk <= p; ++kk) {
@@ -110,7 +114,7 @@ __global__ void k_l2p_f64(size_t n, const int32_t* __restrict__ body_leaf, const
                     uk = d;
                 } else {
                     const double a = (double)(2 * kk - 1) * rz;
-                    uk = zscale(zsub(zscale(u1, a), zscale(u2, r2)), c_tab.invc[kk][l]);
+                    uk = zscale(zsub(zscale(u1, a), zscale(u2, r2)), g_tab.invc[kk][l]);
                     u2 = u1;
                     u1 = uk;
                 }

@@ -14,10 +14,14 @@
 
 namespace fmmx {
 
-static __constant__ OrderTables c_tab;
+// The order tables in global memory: the kernels read them with lane-
+// dependent indices (a lane per order m or per degree), which the constant
+// cache would serialise over the distinct addresses; global loads are served
+// from L1 in parallel.
+static __device__ OrderTables g_tab;
 
 void upload_tables_exact(const OrderTables& t, cudaStream_t s) {
-    cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s);
 }
 
 // ------------------------------------------------------------ bounding box
@@ -530,14 +534,14 @@ __device__ __forceinline__ void split_nm(int e, int& n, int& m) {
 // upsilon_table_into, harmonic.rs:141-173, operation order kept.
 __device__ __forceinline__ void upsilon_column(double dx, double dy, double dz, double r2, int p, int m, zd* u) {
     zd d = mk(1.0, 0.0);
-    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk(dx, dy), c_tab.inv2m[j]), d);
+    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk(dx, dy), g_tab.inv2m[j]), d);
     u[cidx(m, m)] = d;
     zd u1 = d, u2 = mk(0.0, 0.0);
     for (int n = m + 1; n <= p; ++n) {
         double a = (double)(2 * n - 1) * dz;
         zd t = zscale(u1, a);
         if (n >= m + 2) t = zsub(t, zscale(u2, r2));
-        zd un = zscale(t, c_tab.invc[n][m]);
+        zd un = zscale(t, g_tab.invc[n][m]);
         u[cidx(n, m)] = un;
         u2 = u1;
         u1 = un;
@@ -548,55 +552,112 @@ __device__ __forceinline__ void upsilon_column(double dx, double dy, double dz, 
     }
 }
 
+// Shared memory of k_upward_exact per warp: the cell's accumulator (dim
+// complex), then either the Υ table of an M2M child offset (dim complex) or,
+// for a leaf's P2M, the m >= 0 Υ tables of a round of B bodies, entry-major
+// in separate real and imaginary arrays of stride B + 1 (conflict-free both
+// when a lane writes its body's table and when lanes read one body's
+// entries).
+__host__ __device__ size_t upward_exact_smem_per_warp(int p) {
+    const int B = p2m_round(p), H = (p + 1) * (p + 2) / 2;
+    const size_t u = (size_t)dimp(p) * sizeof(zd), tab = 2 * (size_t)H * (B + 1) * sizeof(double);
+    return (size_t)dimp(p) * sizeof(zd) + (u > tab ? u : tab);
+}
+
 // One warp per cell of a level, deepest level first (compute_moments,
 // moments.rs:96-108): P2M for leaves (p2m_cell :30-53), M2M for internal
 // cells (m2m_cell :56-90), then the multipole power (:150-168) and, when f is
-// given, fmin (mac.rs:151-173).
+// given, fmin (mac.rs:151-173). With skip_internal (the engine's choice), the
+// internal cells of the level are left to k_m2m_exact_block.
+//
+// P2M: the lanes build the Υ tables of B bodies at once (a lane per body, the
+// recursion of upsilon_table_into, harmonic.rs:141-173); then each lane owns
+// the m >= 0 coefficients e = lane, lane + 32, ... and adds m_k Υ_k[e] over
+// the round's bodies in slot order, so every coefficient is the reference's
+// sum in the reference's order.
 __global__ void k_upward_exact(const int32_t* __restrict__ level_cells, int lstart, int lcnt, CellsView cells,
                                const double* __restrict__ x, const double* __restrict__ y,
                                const double* __restrict__ z, const double* __restrict__ m, int p,
                                zd* __restrict__ moments, double* __restrict__ pows, const double* __restrict__ f,
-                               double* __restrict__ fmin_out) {
+                               double* __restrict__ fmin_out, int skip_internal) {
     extern __shared__ unsigned char smem_raw[];
     const int dim = dimp(p);
+    const int H = (p + 1) * (p + 2) / 2;
+    const int B = p2m_round(p), S = B + 1;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    zd* u = reinterpret_cast<zd*>(smem_raw) + wib * 2 * dim;
-    zd* acc = u + dim;
+    unsigned char* wbase = smem_raw + (size_t)wib * upward_exact_smem_per_warp(p);
+    zd* acc = reinterpret_cast<zd*>(wbase);
+    zd* u = acc + dim;                                   // M2M: Υ of the child offset
+    double* tre = reinterpret_cast<double*>(acc + dim);  // P2M: Υ tables, real parts
+    double* tim = tre + (size_t)H * S;                   //      imaginary parts
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int j = warp; j < lcnt; j += nwarps) {
         const int c = level_cells[lstart + j];
+        if (skip_internal && !cells.leaf[c]) continue;
         const double zx = cells.cx[c], zy = cells.cy[c], zz = cells.cz[c];
         for (int e = lane; e < dim; e += 32) acc[e] = mk(0.0, 0.0);
         __syncwarp();
         if (cells.leaf[c]) {
             const uint32_t fst = cells.first[c], end = fst + cells.count[c];
-            for (uint32_t k = fst; k < end; ++k) {
-                const double dx = x[k] - zx, dy = y[k] - zy, dz = z[k] - zz;
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                const double mk_ = m[k];
-                for (int mm = lane; mm <= p; mm += 32) {
+            double ar[8], ai[8];  // this lane's coefficients e = lane + 32 t (m >= 0 half, H <= 231)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) ar[t] = ai[t] = 0.0;
+            for (uint32_t k0 = fst; k0 < end; k0 += B) {
+                const int nb = (int)min((uint32_t)B, end - k0);
+                if (lane < nb) {
+                    const uint32_t k = k0 + lane;
+                    const double dx = x[k] - zx, dy = y[k] - zy, dz = z[k] - zz;
+                    const double r2 = dx * dx + dy * dy + dz * dz;
                     zd d = mk(1.0, 0.0);
-                    for (int jj = 1; jj <= mm; ++jj) d = zmul(zscale(mk(dx, dy), c_tab.inv2m[jj]), d);
-                    zd* a0 = &acc[cidx(mm, mm)];
-                    *a0 = zadd(*a0, zscale(d, mk_));
-                    zd u1 = d, u2 = mk(0.0, 0.0);
-                    for (int n = mm + 1; n <= p; ++n) {
-                        double a = (double)(2 * n - 1) * dz;
-                        zd t = zscale(u1, a);
-                        if (n >= mm + 2) t = zsub(t, zscale(u2, r2));
-                        zd un = zscale(t, c_tab.invc[n][mm]);
-                        zd* an = &acc[cidx(n, mm)];
-                        *an = zadd(*an, zscale(un, mk_));
-                        u2 = u1;
-                        u1 = un;
+                    for (int mm = 0; mm <= p; ++mm) {
+                        if (mm > 0) d = zmul(zscale(mk(dx, dy), g_tab.inv2m[mm]), d);
+                        int h = mm * (mm + 1) / 2 + mm;  // half index of (mm, mm)
+                        tre[h * S + lane] = d.re;
+                        tim[h * S + lane] = d.im;
+                        zd u1 = d, u2 = mk(0.0, 0.0);
+                        for (int n = mm + 1; n <= p; ++n) {
+                            const double a = (double)(2 * n - 1) * dz;
+                            zd t = zscale(u1, a);
+                            if (n >= mm + 2) t = zsub(t, zscale(u2, r2));
+                            const zd un = zscale(t, g_tab.invc[n][mm]);
+                            h += n;  // half index of (n, mm)
+                            tre[h * S + lane] = un.re;
+                            tim[h * S + lane] = un.im;
+                            u2 = u1;
+                            u1 = un;
+                        }
                     }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const int e = lane + 32 * t;
+                    if (e < H) {
+                        for (int b = 0; b < nb; ++b) {
+                            const double mk_ = m[k0 + b];
+                            ar[t] += tre[e * S + b] * mk_;
+                            ai[t] += tim[e * S + b] * mk_;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            // the m >= 0 sums into the full layout; negative orders mirror
+            // exactly (every increment of M_n^{-m} is (-1)^m conj of the
+            // M_n^m increment)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int e = lane + 32 * t;
+                if (e < H) {
+                    int n = 0;
+                    while ((n + 1) * (n + 2) / 2 <= e) ++n;
+                    const int mm = e - n * (n + 1) / 2;
+                    acc[cidx(n, mm)] = mk(ar[t], ai[t]);
                 }
             }
             __syncwarp();
-            // Negative orders: every increment of M_n^{-m} is exactly
-            // (-1)^m conj of the M_n^m increment, so the sums mirror exactly.
             for (int e = lane; e < dim; e += 32) {
                 int n, mm;
                 split_nm(e, n, mm);
@@ -636,7 +697,7 @@ __global__ void k_upward_exact(const int32_t* __restrict__ level_cells, int lsta
             for (int mm = -n; mm <= n; ++mm) {
                 int am = mm < 0 ? -mm : mm;
                 zd v = acc[cidx(n, mm)];
-                double w = c_tab.fact[n - am] * c_tab.fact[n + am];
+                double w = g_tab.fact[n - am] * g_tab.fact[n + am];
                 s += w * (v.re * v.re + v.im * v.im);
             }
             pows[(size_t)c * (p + 1) + n] = sqrt(s);
@@ -655,6 +716,84 @@ __global__ void k_upward_exact(const int32_t* __restrict__ level_cells, int lsta
             fmin_out[c] = mn;
         }
         __syncwarp();
+    }
+}
+
+// M2M of the internal cells of a level, one block per cell:
+// the Υ tables of the (up to 8) child offsets and each child's convolution
+// sums s_o[e] (8 dim independent chains) are computed side by side; then
+// every coefficient adds its children's sums in octant order, as m2m_cell
+// (moments.rs:56-90) does one child after the other. Power and fmin as in
+// k_upward_exact. Shared memory: 16 dim complex.
+__global__ void __launch_bounds__(256) k_m2m_exact_block(const int32_t* __restrict__ level_cells, int lstart,
+                                                         int lcnt, CellsView cells, int p, zd* __restrict__ moments,
+                                                         double* __restrict__ pows, const double* __restrict__ f,
+                                                         double* __restrict__ fmin_out) {
+    extern __shared__ unsigned char smem_raw[];
+    const int dim = dimp(p);
+    zd* ut = reinterpret_cast<zd*>(smem_raw);  // 8 Υ tables
+    zd* st = ut + 8 * dim;                      // 8 child sums
+    __shared__ int ch[8];
+    const int tid = threadIdx.x;
+    for (int j = blockIdx.x; j < lcnt; j += gridDim.x) {
+        const int c = level_cells[lstart + j];
+        if (cells.leaf[c]) continue;  // uniform: the whole block skips
+        if (tid < 8) ch[tid] = cells.child[8 * c + tid];
+        __syncthreads();
+        const double zx = cells.cx[c], zy = cells.cy[c], zz = cells.cz[c];
+        for (int t = tid; t < 8 * (p + 1); t += blockDim.x) {
+            const int o = t / (p + 1), mm = t % (p + 1);
+            const int cc = ch[o];
+            if (cc < 0) continue;
+            const double dx = cells.cx[cc] - zx, dy = cells.cy[cc] - zy, dz = cells.cz[cc] - zz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            upsilon_column(dx, dy, dz, r2, p, mm, ut + o * dim);
+        }
+        __syncthreads();
+        for (int t = tid; t < 8 * dim; t += blockDim.x) {
+            const int o = t / dim, e = t % dim;
+            const int cc = ch[o];
+            if (cc < 0) continue;
+            int n, mm;
+            split_nm(e, n, mm);
+            const zd* u = ut + o * dim;
+            const zd* mc = moments + (size_t)cc * dim;
+            zd s = mk(0.0, 0.0);
+            for (int k = 0; k <= n; ++k) {
+                const int nk = n - k;
+                const int lo = max(-k, mm - nk), hi = min(k, mm + nk);
+                for (int l = lo; l <= hi; ++l) s = zadd(s, zmul(u[cidx(k, l)], mc[cidx(nk, mm - l)]));
+            }
+            st[o * dim + e] = s;
+        }
+        __syncthreads();
+        zd* out = moments + (size_t)c * dim;
+        zd* acc = ut;  // the tables are no longer needed: the sums land in slot 0
+        for (int e = tid; e < dim; e += blockDim.x) {
+            zd a = mk(0.0, 0.0);
+            for (int o = 0; o < 8; ++o)
+                if (ch[o] >= 0) a = zadd(a, st[o * dim + e]);
+            out[e] = a;
+            acc[e] = a;
+        }
+        __syncthreads();
+        for (int n = tid; n <= p; n += blockDim.x) {
+            double s = 0.0;
+            for (int mm = -n; mm <= n; ++mm) {
+                int am = mm < 0 ? -mm : mm;
+                zd v = acc[cidx(n, mm)];
+                double w = g_tab.fact[n - am] * g_tab.fact[n + am];
+                s += w * (v.re * v.re + v.im * v.im);
+            }
+            pows[(size_t)c * (p + 1) + n] = sqrt(s);
+        }
+        if (f != nullptr && tid == 0) {
+            double mn = INFINITY;
+            for (int o = 0; o < 8; ++o)
+                if (ch[o] >= 0) mn = fmin(mn, fmin_out[ch[o]]);
+            fmin_out[c] = mn;
+        }
+        __syncthreads();
     }
 }
 
@@ -747,7 +886,7 @@ __device__ __forceinline__ bool accept_dehnen(const CellsView& cv, const MacPara
     for (int j = 1; j <= p; ++j) rpows[j] = rpows[j - 1] * rb;
     const double* pw = pows + (size_t)a * (p + 1);
     double s = 0.0;
-    for (int k = 0; k <= p; ++k) s += c_tab.binom[p][k] * pw[k] * rpows[p - k];
+    for (int k = 0; k <= p; ++k) s += g_tab.binom[p][k] * pw[k] * rpows[p - k];
     const double ma = cv.mass[a];
     const double e = s / (ma * rp);
     const double denom = ra + rb;

@@ -29,8 +29,8 @@ extern "C" {
 /* Status codes. FMMX_OVER_BUDGET is the reference GPU backend's OverBudget
  * (crates/visual/src/gpufmm.rs:1653-1672): an engine buffer would take the
  * context above its device_budget_bytes; the message names the buffer, the
- * bytes and the limit, and the context stays usable (the caller can retry
- * smaller or fall back). FMMX_LEAF_OVERFLOW mirrors the reference's
+ * bytes and the limit; the context then drops its cached device buffers
+ * and stays usable (the caller can retry smaller or fall back). FMMX_LEAF_OVERFLOW mirrors the reference's
  * OverfullLeaf (gpufmm.rs:1377-1379, a leaf above its 64-lane kernels); no
  * kernel here bounds the bodies of a leaf, so it is never returned. */
 typedef enum fmmx_status {
