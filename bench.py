@@ -938,7 +938,7 @@ def run_serve(args, cfg, rank, world, local_rank):
             v = np.zeros_like(p)
         sessions.append(Session(sid=i, mass=m, pos=p, vel=v, steps=args.serve_steps, dt=1e-3, arrival=float(t)))
     kw = dict(p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"], n_leaf=cfg["n_leaf"],
-              precision=args.precision, budget_bytes=args.budget_gb * 1e9)
+              precision=args.precision, budget_bytes=args.budget_gb * 1e9, refresh_every=args.refresh_every)
     srv = Server(**kw, latency_slo=args.latency_slo)  # calibrates the isolated step time first
     srv.start()  # every lane on its own thread and stream
     t0 = time.perf_counter()
@@ -971,13 +971,20 @@ def run_serve(args, cfg, rank, world, local_rank):
                        "mix_p50_ms": float(np.percentile(s.step_ms, 50)), "mix_max_ms": float(np.max(s.step_ms)),
                        "steps_over_2x": int(np.sum(np.asarray(s.step_ms) > 2 * a50)), "steps": len(s.step_ms)})
     rr = [r["mix_p99_ms"] / max(r["alone_p50_ms"], 1e-6) for r in ratios]
+    # batching: sessions per tick of the ticks that stepped a batch (trace field 6: members)
+    per_tick = [t[6] for ln in srv.lanes for t in ln.trace]
+    batching = {"ticks": len(per_tick),
+                "sessions_per_tick_mean": float(np.mean(per_tick)) if per_tick else 0.0,
+                "ticks_with_more_than_one": float(np.mean([m > 1 for m in per_tick])) if per_tick else 0.0,
+                "sessions_per_tick_max": int(max(per_tick)) if per_tick else 0}
     line = {"metric": METRIC, "value": rep["bodies_per_s"], "unit": "bodies/s", "n_gpus": 1, "steps": rep["ticks"],
             "warmup": 0, "ms_per_step": rep["step_ms_p50"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
             "dtype": "f64" if args.precision == "plain" else "f32+f64",
             "config": {"workload": f"serving: Poisson {args.rate}/s for {args.duration}s, N log-uniform[1e3,"
-                                   f"{args.serve_nmax:.0e}], {args.serve_steps} KDK steps", "budget_gb": args.budget_gb},
-            "serve": {**rep, "wall_s": wall, "arrived": len(sessions), "submitted": k,
+                                   f"{args.serve_nmax:.0e}], {args.serve_steps} KDK steps", "budget_gb": args.budget_gb,
+                       "refresh_every": args.refresh_every},
+            "serve": {**rep, "wall_s": wall, "arrived": len(sessions), "submitted": k, "batching": batching,
                       "queued_at_end": len(srv.queue), "active_at_end": len(srv.active),
                       "admitted_sessions_mean": float(np.mean([o[0] for o in occ])) if occ else 0.0,
                       "admitted_bodies_mean": float(np.mean([o[1] for o in occ])) if occ else 0.0,
@@ -1004,7 +1011,7 @@ def main():
     ap.add_argument("--nsys", type=int, default=512)
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--rate", type=float, default=50.0)
-    ap.add_argument("--duration", type=float, default=10.0)
+    ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--drain", type=float, default=20.0)
     ap.add_argument("--serve-steps", type=int, default=100)
     ap.add_argument("--serve-nmax", type=float, default=1e6)

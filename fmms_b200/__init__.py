@@ -123,6 +123,7 @@ SIGNATURES = {
     "fmmx_build_device": (_st, [_vp, _sz, _vp, _vp]),
     "fmmx_evaluate_device": (_st, [_vp, _vp, _vp, _vp, _vp]),
     "fmmx_synchronize": (_st, [_vp]),
+    "fmmx_kdk_step_device": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _u64p, C.c_int]),
     "fmmx_leapfrog_device": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, C.c_int, C.c_int]),
     "fmmx_build_ensemble": (_st, [_vp, _sz, _u64p, _dp, _dp]),
     "fmmx_build_ensemble_device": (_st, [_vp, _sz, _u64p, _vp, _vp]),
@@ -309,6 +310,18 @@ class Fmm:
         sc = {"kdk": 0, "dkd": 1}[scheme]
         self._check(lib().fmmx_leapfrog_device(self._h, pos_ptr, vel_ptr, mass_ptr, acc_ptr, pot_ptr, float(dt),
                                                int(nsteps), sc, int(refresh_every)))
+
+    def kdk_step_device(self, pos_ptr, vel_ptr, mass_ptr, acc_ptr, pot_ptr, dt_ptr, offsets=None,
+                        rebuild=True):
+        """One kick-drift-kick step with a time step per body (device array of
+        n FP64; 0 keeps a body in place). With offsets the tree is rebuilt over
+        those systems; without, rebuild=False reuses the last tree and lists."""
+        off = None if offsets is None else np.ascontiguousarray(offsets, dtype=np.uint64)
+        if off is not None:
+            self.n = int(off[-1])
+        self._check(lib().fmmx_kdk_step_device(self._h, pos_ptr, vel_ptr, mass_ptr, acc_ptr, pot_ptr, dt_ptr,
+                                               0 if off is None else len(off) - 1,
+                                               None if off is None else _ptr(off, _u64p), 1 if rebuild else 0))
 
     def synchronize(self):
         self._check(lib().fmmx_synchronize(self._h))

@@ -1336,6 +1336,50 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, co
     return FMMX_OK;
 }
 
+fmmx_status fmmx_kdk_step_device(fmmx_ctx* ctx, double* d_pos, double* d_vel, const double* d_mass, double* d_acc,
+                                 double* d_pot, const double* d_dt, size_t nsys, const uint64_t* offsets,
+                                 int rebuild) {
+    if (!ctx) return FMMX_INVALID_ARG;
+    BudgetScope bscope(&ctx->budget);
+    if (!d_pos || !d_vel || !d_mass || !d_acc || !d_dt) return fail(ctx, FMMX_INVALID_ARG, "null pointer");
+    if (!offsets && !ctx->built) return fail(ctx, FMMX_NOT_BUILT, "no tree to step on: give offsets");
+    if (offsets && (nsys == 0 || nsys > (1u << 24))) return fail(ctx, FMMX_INVALID_ARG, "bad system count");
+    cudaSetDevice(ctx->cfg.device);
+    cudaStream_t s = ctx->stream;
+    const size_t n = offsets ? (size_t)offsets[nsys] : ctx->n;
+    if (n == 0) return fail(ctx, FMMX_INVALID_ARG, "empty input");
+    if (!d_pot) {
+        if (ctx->pot_out.ensure(n) != cudaSuccess) return fail(ctx, FMMX_OUT_OF_MEMORY, "pot buffer");
+        d_pot = ctx->pot_out.p;
+    }
+    const unsigned g = grid_for(3 * n, 256);
+    k_kick_rows<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, d_dt, 0.5);
+    k_drift_rows<<<g, 256, 0, s>>>(3 * n, d_pos, d_vel, d_dt);
+    if (cudaGetLastError() != cudaSuccess) return fail(ctx, FMMX_DEVICE_ERROR, "kick/drift");
+    fmmx_status st = FMMX_OK;
+    const bool build = offsets != nullptr || rebuild || !ctx->lists_valid;
+    if (build) {
+        if (offsets) {
+            st = nsys == 1 ? build_impl(ctx, n, d_pos, d_mass) : build_impl(ctx, n, d_pos, d_mass, (int)nsys, offsets);
+        } else if (ctx->nsys == 1) {
+            st = build_impl(ctx, n, d_pos, d_mass);
+        } else {
+            std::vector<uint64_t> off(ctx->sys_off_host);
+            st = build_impl(ctx, n, d_pos, d_mass, ctx->nsys, off.data());
+        }
+        if (st != FMMX_OK) return finish(ctx, st);
+        ctx->steps_since_build = 0;
+        st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, false);
+    } else {
+        ctx->steps_since_build++;
+        st = evaluate_impl(ctx, d_pos, d_mass, d_acc, d_pot, true);
+    }
+    if (st != FMMX_OK) return finish(ctx, st);
+    k_kick_rows<<<g, 256, 0, s>>>(3 * n, d_vel, d_acc, d_dt, 0.5);
+    if (cudaGetLastError() != cudaSuccess) return fail(ctx, FMMX_DEVICE_ERROR, "kick");
+    return FMMX_OK;
+}
+
 fmmx_status fmmx_evaluate(fmmx_ctx* ctx, const double* pos, const double* mass, double* acc, double* pot) {
     if (!ctx) return FMMX_INVALID_ARG;
     BudgetScope bscope(&ctx->budget);

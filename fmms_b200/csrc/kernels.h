@@ -173,6 +173,8 @@ __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, 
 // integrate.cu
 __global__ void k_kick(size_t n3, double* v, const double* a, double h);
 __global__ void k_drift(size_t n3, double* x, const double* v, double h);
+__global__ void k_kick_rows(size_t n3, double* v, const double* a, const double* dt, double c);
+__global__ void k_drift_rows(size_t n3, double* x, const double* v, const double* dt);
 
 // direct.cu
 __global__ void k_direct_targets(const double* pos, const double* mass, size_t n, const uint32_t* tgt, size_t nt,

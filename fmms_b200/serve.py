@@ -286,6 +286,8 @@ class Lane:
         self.departures = 0  # sessions finished in this lane
         self.evictions = 0  # joins undone because the joining tick broke the bound
         self.t_built = 0.0
+        self.forest_dirty = True  # the members changed since the forest was built
+        self.ticks_on_tree = 0  # ticks stepped on the current forest's tree and lists
         # one record per tick (TickRecord fields), for latency analysis
         self.trace: deque[tuple] = deque(maxlen=1 << 17)
 
@@ -300,11 +302,6 @@ class Lane:
 
     def bodies(self):
         return sum(s.n for s in self.members)
-
-    def evaluate(self, pos, mass, acc, pot, offsets):
-        self.fmm.build_ensemble_device(offsets, pos.data_ptr(), mass.data_ptr())
-        self.t_built = time.perf_counter()
-        self.fmm.evaluate_device(pos.data_ptr(), mass.data_ptr(), acc.data_ptr(), pot.data_ptr())
 
     # ---------------------------------------------------------------- admission
     def admit(self, now):
@@ -358,6 +355,7 @@ class Lane:
         rows = [pos, vel, acc, pot, mass]
         self.state = rows if self.state is None else [torch.cat([a, b]) for a, b in zip(self.state, rows)]
         self.members.extend(new)
+        self.forest_dirty = True
         self._set_dts()
 
     def _set_dts(self):
@@ -389,6 +387,7 @@ class Lane:
             self.queue.appendleft(s)
         self.evictions += len(sessions)
         self.predicted_ms = None
+        self.forest_dirty = True
         self._set_dts()
 
     def leave(self, now):
@@ -425,6 +424,7 @@ class Lane:
         if changed:
             idx = torch.cat(rows)
             self.state = [t.index_select(0, idx) for t in self.state]
+            self.forest_dirty = True
         return changed
 
     # ---------------------------------------------------------------- one tick
@@ -442,14 +442,19 @@ class Lane:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(self.stream)
-            if stepping:
-                vel.add_(0.5 * self.dts * acc)
-                pos.add_(self.dts * vel)
+            # one engine call: kick and drift with per-row time steps (0 for
+            # joining rows), the forest build -- over the new members when they
+            # changed, else every refresh_every ticks, in between the tree and
+            # lists are reused -- the evaluation and the closing kick
+            rebuild = self.forest_dirty or self.ticks_on_tree + 1 >= self.srv.refresh_every
+            offsets = self.offsets(self.members) if self.forest_dirty else None
             t_kd = time.perf_counter()
-            self.evaluate(pos, mass, acc, pot, self.offsets(self.members))
+            self.fmm.kdk_step_device(pos.data_ptr(), vel.data_ptr(), mass.data_ptr(), acc.data_ptr(),
+                                     pot.data_ptr(), self.dts.data_ptr(), offsets, rebuild)
+            self.t_built = t_kd
+            self.forest_dirty = False
+            self.ticks_on_tree = 0 if rebuild else self.ticks_on_tree + 1
             t_ev = time.perf_counter()
-            if stepping:
-                vel.add_(0.5 * self.dts * acc)
             t_launched = time.perf_counter()
             e1.record(self.stream)
             if self.srv.lanes[0] is self:
@@ -508,11 +513,16 @@ class Server:
     their admission (sessions beyond it are staged when they join); also the
     allocator pool reserved on the copy stream.
     lane_reserve_bytes: allocator pool reserved on each lane's stream.
+    refresh_every: a lane's forest is rebuilt whenever its members change and
+    otherwise every refresh_every ticks; in between the tree and interaction
+    lists are reused (1, the default: every tick, which keeps each session's
+    result bitwise the one it gets alone; above 1 a session's rebuild times
+    depend on its neighbours' arrivals and departures).
     """
 
     def __init__(self, *, p=8, theta=0.5, softening=1e-3, n_leaf=64, precision="mixed", budget_bytes=160e9,
                  lanes=LANE_BOUNDS, device=0, latency_slo=None, headroom=None, model=None, max_bypass_s=2.0,
-                 scan=256, stage_limit_bytes=8e9, lane_reserve_bytes=2e9):
+                 scan=256, stage_limit_bytes=8e9, lane_reserve_bytes=2e9, refresh_every=1):
         import torch
 
         import fmms_b200 as fx
@@ -523,6 +533,7 @@ class Server:
         self.dev = f"cuda:{device}"
         torch.cuda.set_device(device)
         self.p, self.theta, self.softening, self.n_leaf, self.precision = p, theta, softening, n_leaf, precision
+        self.refresh_every = max(1, int(refresh_every))
         self.budget = float(budget_bytes)
         self.used = 0.0
         self.staged_bytes = 0.0

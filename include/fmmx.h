@@ -173,6 +173,21 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos_xyz, double* d_vel
                                  double* d_acc_xyz, double* d_pot, double dt, int nsteps, int scheme,
                                  int refresh_every);
 
+/* One kick-drift-kick step with a time step per body (d_dt[n]; a body with
+ * dt = 0 does not move: its forces are evaluated, as for a session joining a
+ * serving batch). On entry d_acc holds the forces at d_pos of the bodies with
+ * dt > 0. With offsets (host, nsys + 1 entries, as fmmx_build_ensemble) the
+ * tree is rebuilt over those systems from the drifted positions; without,
+ * over the systems of the last build when rebuild != 0 (or when there are no
+ * lists yet), else the tree and interaction lists of the last evaluation are
+ * reused and only moments and locals are recomputed (tree reuse,
+ * crates/visual/src/gpufmm.rs:9-20). Queued on the context's stream; returns
+ * once the step is queued. No reference counterpart as a library call (the
+ * reference's loops step on the host, crates/fmm/tests/energy_gate.rs:156-177). */
+fmmx_status fmmx_kdk_step_device(fmmx_ctx* ctx, double* d_pos_xyz, double* d_vel_xyz, const double* d_mass,
+                                 double* d_acc_xyz, double* d_pot, const double* d_dt, size_t nsys,
+                                 const uint64_t* offsets, int rebuild);
+
 /* Wait for the context's stream. */
 fmmx_status fmmx_synchronize(fmmx_ctx* ctx);
 

@@ -224,3 +224,42 @@ def test_energy_gate_mixed(orc):
     assert abs(slope) < 1e-6, slope
     assert max(abs(w) for w in windows) < 1e-3, windows
     assert momentum_rel(mass, v) < 1e-6
+
+
+@pytest.mark.parametrize("refresh", [1, 3])
+def test_kdk_step_rows(refresh):
+    """fmmx_kdk_step_device with the same time step on every row gives the
+    bits of fmmx_leapfrog_device (KDK, same refresh cadence, graphs off); rows
+    with a zero step keep their positions and velocities exactly."""
+    import torch
+
+    import fmms_b200 as fx
+
+    mass, pos, vel = fx.gen_plummer_ic(6000, seed=13)
+    n = len(mass)
+    kw = dict(p=8, eps=0.0, n_leaf=32, mac="theta", theta=0.5, softening=1e-3, precision="mixed", use_graphs=False)
+    x1, v1, a1, _ = run_leapfrog(mass, pos, vel, kw, 1e-3, 6, "kdk", refresh)
+    d_pos = torch.from_numpy(pos.copy()).cuda()
+    d_vel = torch.from_numpy(vel.copy()).cuda()
+    d_mass = torch.from_numpy(mass).cuda()
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_dt = torch.full((n,), 1e-3, dtype=torch.float64, device="cuda")
+    g = fx.Fmm(None, None, **kw, stream=torch.cuda.current_stream().cuda_stream)
+    g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
+    g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
+    ptrs = (d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr(), d_dt.data_ptr())
+    for k in range(6):
+        g.kdk_step_device(*ptrs, rebuild=(k + 1) % refresh == 0)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_pos.cpu().numpy(), x1) and np.array_equal(d_vel.cpu().numpy(), v1)
+    assert np.array_equal(d_acc.cpu().numpy(), a1)
+    # a zero step on the second half of the rows: those bodies stay put
+    x0, v0 = d_pos.cpu().numpy(), d_vel.cpu().numpy()
+    d_dt[n // 2:] = 0.0
+    g.kdk_step_device(*ptrs, offsets=np.array([0, n], dtype=np.uint64))
+    torch.cuda.synchronize()
+    xa, va = d_pos.cpu().numpy(), d_vel.cpu().numpy()
+    assert np.array_equal(xa[n // 2:], x0[n // 2:]) and np.array_equal(va[n // 2:], v0[n // 2:])
+    assert not np.array_equal(xa[: n // 2], x0[: n // 2])
+    g.close()

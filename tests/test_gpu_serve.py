@@ -62,3 +62,24 @@ def test_admission_respects_budget():
         peak = max(peak, srv.mem_used())
         assert srv.mem_used() <= budget
     assert len(srv.done) == 4 and peak > 0
+
+
+def test_forest_tree_reuse_in_serving():
+    """refresh_every 3: a lane keeps its forest's tree and lists for up to 3
+    ticks while its members do not change. Each session's trajectory stays
+    within the FMM's force error of the one it gets alone (their rebuild times
+    differ), and every session completes its steps."""
+    from fmms_b200.serve import Server, run_session_alone
+
+    kw = dict(p=8, theta=0.5, softening=1e-3, n_leaf=64, precision="mixed", refresh_every=3)
+    sess = make_sessions()
+    srv = Server(**kw)
+    for s in sess:
+        srv.submit(s)
+    srv.run_until_idle()
+    assert len(srv.done) == len(sess)
+    for s in srv.done:
+        assert len(s.step_ms) == s.steps
+        pa, va, _ = run_session_alone(s, **kw)
+        scale = np.abs(pa).max()
+        assert np.max(np.abs(s.result_pos - pa)) < 1e-7 * scale
