@@ -861,19 +861,19 @@ def run_ensemble(args, cfg, rank, world, local_rank):
     pos = np.concatenate([p for _, p in parts])
     n = len(mass)
     tune = None
-    n_leaf, p_use, tile = cfg["n_leaf"], cfg["p"], 0
+    n_leaf, p_use, tile, theta, gap = cfg["n_leaf"], cfg["p"], 0, cfg["theta"], 0.0
     if args.autotune:
         from fmms_b200.autotune import tune_ensemble
 
         tune = tune_ensemble(parts, p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"],
                              precision=args.precision, device=dev)
-        n_leaf, p_use, tile = tune["n_leaf"], tune["p"], tune["p2p_tile"]
+        n_leaf, p_use, tile, theta, gap = tune["n_leaf"], tune["p"], tune["p2p_tile"], tune["theta"], tune["soft_gap"]
     d_pos = torch.from_numpy(pos).to(f"cuda:{dev}")
     d_mass = torch.from_numpy(mass).to(f"cuda:{dev}")
     d_acc = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{dev}")
     d_pot = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
-    g = fx.Fmm(None, None, p_use, 0.0, n_leaf, mac="theta", theta=cfg["theta"], softening=cfg["softening"],
-               precision=args.precision, device=dev, stream=stream.cuda_stream, p2p_tile=tile)
+    g = fx.Fmm(None, None, p_use, 0.0, n_leaf, mac="theta", theta=theta, softening=cfg["softening"],
+               precision=args.precision, device=dev, stream=stream.cuda_stream, p2p_tile=tile, soft_gap=gap)
 
     def step():
         g.build_ensemble_device(off, d_pos.data_ptr(), d_mass.data_ptr())
@@ -907,9 +907,11 @@ def run_ensemble(args, cfg, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "data": "synthetic", "dtype": "f64" if args.precision == "plain" else "f32+f64",
             "config": {"workload": f"{args.nsys} Plummer systems, N log-uniform[1e3,1e5] (total {n}), one forest",
-                       "p": p_use, "n_leaf": n_leaf, "p2p_tile": tile,
+                       "p": p_use, "n_leaf": n_leaf, "p2p_tile": tile, "theta": theta, "soft_gap": gap,
                        "autotune": {k: v for k, v in (tune or {}).items() if k != "candidates"}},
-            "per_system_force_err_p99": {"median": float(np.median(p99s)), "max": float(np.max(p99s))},
+            "per_system_force_err_p99": {"median": float(np.median(p99s)), "max": float(np.max(p99s)),
+                                         "systems_over_1e-5": int(np.sum(np.asarray(p99s) > 1e-5))},
+            "launches_per_evaluation": int(st["kernel_launches"]),
             "stages_ms": {k[3:]: round(v, 3) for k, v in st.items() if k.startswith("ms_")},
             "gpu_launches": int(st["kernel_launches"]) * args.steps}
     print(json.dumps(line), flush=True)

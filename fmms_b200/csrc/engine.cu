@@ -201,6 +201,7 @@ struct fmmx_ctx {
     // mixed form: normalised FP32 half-layout expansions and the per-cell length
     DBuf<zf> mom_f, loc_f;
     DBuf<double> ell;
+    DBuf<unsigned long long> rho_now;  // radii about the build's centres on a reused tree (FP64 bits)
     DBuf<float> ellf;
 
     // walk
@@ -849,7 +850,23 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CK(ctx->loc_f.ensure((size_t)nc * half_stride(p)), "alloc expansions");
         CK(ctx->ell.ensure(nc), "alloc expansions");
         CK(ctx->ellf.ensure(nc), "alloc expansions");
-        k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, ctx->c_rho.p, ctx->c_h.p, ctx->ell.p, ctx->ellf.p);
+        const double* rho = ctx->c_rho.p;
+        // sized on every mixed evaluation, so that a reuse step recorded into
+        // a CUDA graph never allocates while capturing
+        CK(ctx->rho_now.ensure(nc), "alloc expansions");
+        if (reuse) {  // the bodies moved since the build: radii about the same centres
+            CK(cudaMemsetAsync(ctx->rho_now.p, 0, (size_t)nc * sizeof(unsigned long long), s), "memset");
+            k_rho_bodies<<<grid_for(n, 256), 256, 0, s>>>(n, ctx->body_leaf.p, cv, ctx->x.p, ctx->y.p, ctx->z.p,
+                                                          ctx->rho_now.p);
+            for (int L = ctx->nlevels - 1; L >= 0; --L) {
+                const int cnt = ctx->lvl_count[L];
+                k_rho_level<<<grid_for(cnt, 256), 256, 0, s>>>(ctx->level_cells.p, ctx->lvl_start[L], cnt, cv,
+                                                               ctx->rho_now.p);
+            }
+            LCOUNT(1 + ctx->nlevels);
+            rho = reinterpret_cast<const double*>(ctx->rho_now.p);
+        }
+        k_cell_scale<<<grid_for(nc, 256), 256, 0, s>>>(nc, rho, ctx->c_h.p, ctx->ell.p, ctx->ellf.p);
         LCOUNT(1);
     }
     // the second stream starts once the bodies are gathered (and, for the

@@ -140,6 +140,10 @@ __global__ void k_l2p_f64(size_t n, const int32_t* body_leaf, const uint32_t* or
 // mixed.cu
 void upload_tables_mixed(const OrderTables& t, cudaStream_t s);
 __global__ void k_cell_scale(int nc, const double* rho, const double* h, double* ell, float* ellf);
+__global__ void k_rho_bodies(size_t n, const int32_t* body_leaf, CellsView cv, const double* x, const double* y,
+                             const double* z, unsigned long long* rho_bits);
+__global__ void k_rho_level(const int32_t* level_cells, int lstart, int lcnt, CellsView cv,
+                            unsigned long long* rho_bits);
 __global__ void k_moments_to_mixed(int nc, int p, const zd* full, const double* ell, zf* half);
 void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, const int32_t* level_cells,
                          int lstart, int lcnt, CellsView cv, const double* ell, const double* x, const double* y,

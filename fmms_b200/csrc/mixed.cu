@@ -77,6 +77,41 @@ __global__ void k_cell_scale(int nc, const double* __restrict__ rho, const doubl
     }
 }
 
+// Cell radii about the build's centres for the current positions, on a
+// reused tree: the bodies have drifted since the build, and a cell whose built
+// radius is tiny (a tight pair) would otherwise normalise its moments by a
+// length far below the bodies' distances from its centre, overflowing FP32
+// (M_n / l^n). Never below the built radius. Leaves from their bodies (an
+// atomic max on the bit pattern, which orders like the value for
+// non-negative doubles), internal cells from their children, deepest level
+// first (the construction of tree.rs:152-227 with the centres held fixed).
+__global__ void k_rho_bodies(size_t n, const int32_t* __restrict__ body_leaf, CellsView cv,
+                             const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, unsigned long long* __restrict__ rho_bits) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int c = body_leaf[k];
+        const double dx = x[k] - cv.cx[c], dy = y[k] - cv.cy[c], dz = z[k] - cv.cz[c];
+        const double d = sqrt(dx * dx + dy * dy + dz * dz);
+        atomicMax(rho_bits + c, (unsigned long long)__double_as_longlong(d));
+    }
+}
+__global__ void k_rho_level(const int32_t* __restrict__ level_cells, int lstart, int lcnt, CellsView cv,
+                            unsigned long long* __restrict__ rho_bits) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < lcnt; j += gridDim.x * blockDim.x) {
+        const int c = level_cells[lstart + j];
+        double r = fmax(cv.rho[c], __longlong_as_double((long long)rho_bits[c]));
+        if (!cv.leaf[c]) {
+            for (int o = 0; o < 8; ++o) {
+                const int ch = cv.child[8 * c + o];
+                if (ch < 0) continue;
+                const double dx = cv.cx[ch] - cv.cx[c], dy = cv.cy[ch] - cv.cy[c], dz = cv.cz[ch] - cv.cz[c];
+                r = fmax(r, __longlong_as_double((long long)rho_bits[ch]) + sqrt(dx * dx + dy * dy + dz * dz));
+            }
+        }
+        rho_bits[c] = (unsigned long long)__double_as_longlong(r);
+    }
+}
+
 // FP64 full-layout moments (the exact upward pass) -> normalised FP32 half layout.
 __global__ void k_moments_to_mixed(int nc, int p, const zd* __restrict__ full, const double* __restrict__ ell,
                                    zf* __restrict__ half) {

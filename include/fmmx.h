@@ -181,8 +181,11 @@ fmmx_status fmmx_leapfrog_device(fmmx_ctx* ctx, double* d_pos_xyz, double* d_vel
  * over the systems of the last build when rebuild != 0 (or when there are no
  * lists yet), else the tree and interaction lists of the last evaluation are
  * reused and only moments and locals are recomputed (tree reuse,
- * crates/visual/src/gpufmm.rs:9-20). Queued on the context's stream; returns
- * once the step is queued. No reference counterpart as a library call (the
+ * crates/visual/src/gpufmm.rs:9-20). Runs on the context's stream: returns
+ * once the evaluation has finished on the device (the evaluation reads its
+ * status back), with the closing half kick still queued behind it; a rebuild
+ * also waits for the tree's level counts. No reference counterpart as a
+ * library call (the
  * reference's loops step on the host, crates/fmm/tests/energy_gate.rs:156-177). */
 fmmx_status fmmx_kdk_step_device(fmmx_ctx* ctx, double* d_pos_xyz, double* d_vel_xyz, const double* d_mass,
                                  double* d_acc_xyz, double* d_pot, const double* d_dt, size_t nsys,

@@ -108,6 +108,29 @@ def test_kdk_matches_host_loop(precision, refresh):
     assert np.percentile(rel, 99) < (1e-11 if refresh == 1 else 1e-4)
 
 
+@pytest.mark.parametrize("use_graphs", [False, True])
+def test_mixed_reuse_after_drift_stays_finite(use_graphs):
+    """Mixed form, leaves of 64 and a tree reused for 4 steps while the bodies
+    drift: a cell whose built radius is tiny (a tight pair) must be normalised
+    with its radius about the build's centre at the current positions, else
+    its FP32 moments overflow. The forces stay finite and within the FMM error
+    of the same steps with a rebuild every step."""
+    import torch
+
+    import fmms_b200 as fx
+
+    mass, pos, vel = fx.gen_plummer_ic(3000, seed=50)
+    kw = dict(p=8, eps=0.0, n_leaf=64, mac="theta", theta=0.5, softening=1e-3, precision="mixed",
+              use_graphs=use_graphs)
+    with torch.cuda.stream(torch.cuda.Stream()):  # graphs are recorded on a non-default stream only
+        x4, v4, a4, p4 = run_leapfrog(mass, pos, vel, kw, 1e-3, 4, "kdk", 8)
+        x1, v1, a1, p1 = run_leapfrog(mass, pos, vel, kw, 1e-3, 4, "kdk", 1)
+    assert np.all(np.isfinite(a4)) and np.all(np.isfinite(x4)) and np.all(np.isfinite(p4))
+    rel = np.linalg.norm(a4 - a1, axis=1) / np.linalg.norm(a1, axis=1)
+    assert np.percentile(rel, 99) < 1e-4
+    assert np.max(np.abs(x4 - x1)) < 1e-6 * np.abs(x1).max()
+
+
 @pytest.mark.parametrize("precision", ["plain", "mixed"])
 def test_graph_replay_matches_launches(precision):
     """Steps on a reused tree replayed from a CUDA graph give the bits of the
@@ -238,14 +261,21 @@ def test_kdk_step_rows(refresh):
     mass, pos, vel = fx.gen_plummer_ic(6000, seed=13)
     n = len(mass)
     kw = dict(p=8, eps=0.0, n_leaf=32, mac="theta", theta=0.5, softening=1e-3, precision="mixed", use_graphs=False)
-    x1, v1, a1, _ = run_leapfrog(mass, pos, vel, kw, 1e-3, 6, "kdk", refresh)
+    side = torch.cuda.Stream()  # torch's work and the engine's on one stream
+    with torch.cuda.stream(side):
+        x1, v1, a1, _ = run_leapfrog(mass, pos, vel, kw, 1e-3, 6, "kdk", refresh)
+        kdk_rows_run(fx, torch, side, mass, pos, vel, kw, refresh, x1, v1, a1)
+
+
+def kdk_rows_run(fx, torch, side, mass, pos, vel, kw, refresh, x1, v1, a1):
+    n = len(mass)
     d_pos = torch.from_numpy(pos.copy()).cuda()
     d_vel = torch.from_numpy(vel.copy()).cuda()
     d_mass = torch.from_numpy(mass).cuda()
     d_acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
     d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
     d_dt = torch.full((n,), 1e-3, dtype=torch.float64, device="cuda")
-    g = fx.Fmm(None, None, **kw, stream=torch.cuda.current_stream().cuda_stream)
+    g = fx.Fmm(None, None, **kw, stream=side.cuda_stream)
     g.build_device(d_pos.data_ptr(), d_mass.data_ptr(), n)
     g.evaluate_device(d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr())
     ptrs = (d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr(), d_dt.data_ptr())
