@@ -221,6 +221,7 @@ struct fmmx_ctx {
     // near-field work units of the mixed P2P (per leaf: units, scratch bodies)
     DBuf<uint32_t> p2p_units, p2p_scr, p2p_uoff, p2p_soff;
     DBuf<double4> p2p_part;
+    DBuf<float4> body_loc;  // mixed near field: bodies relative to their leaf's centre, FP32, with the mass
     DBuf<unsigned> p2p_next;
 
     DBuf<int> work;  // persistent-kernel work counter
@@ -778,8 +779,9 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
     CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
     const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_soff.p, ctx->p2p_part.p, ctx->p2p_next.p};
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, ctx->nsm, s2, lp, nc, cv, units,
-                     ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2, ctx->nax.p, ctx->nay.p, ctx->naz.p, ctx->npot.p);
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, ctx->nsm, s2, lp, nc, cv, units, n,
+                     ctx->body_leaf.p, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, ctx->body_loc.p, soft2, ctx->nax.p,
+                     ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s2), "event");
     CK(cudaEventRecord(ctx->fork[2], s2), "event");
@@ -796,7 +798,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
         CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, work, ctx->nsm, s), "m2l");
     }
     if (tm) CK(cudaEventRecord(ev[6], s), "event");
-    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 3);  // m2l, l2l per level, p2p + combine, l2p
+    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 4);  // m2l, l2l per level, coords + p2p + combine, l2p
     for (int L = 1; L < ctx->nlevels; ++L) {
         const int cnt = ctx->lvl_count[L];
         const unsigned g = std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm);
@@ -846,6 +848,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     const int H = (p + 1) * (p + 2) / 2;
     const CellsView cv = view(ctx);
     if (mixed) {
+        CK(ctx->body_loc.ensure(n), "alloc expansions");
         CK(ctx->mom_f.ensure((size_t)nc * half_stride(p)), "alloc expansions");
         CK(ctx->loc_f.ensure((size_t)nc * half_stride(p)), "alloc expansions");
         CK(ctx->ell.ensure(nc), "alloc expansions");

@@ -166,9 +166,10 @@ struct P2pUnits {
 };
 void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
                      uint32_t* scratch);
-void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
-                      const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
-                      double* ay, double* az, double* pot);
+// loc: n float4 of scratch (bodies relative to their leaf's centre, with the mass)
+void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, size_t n,
+                      const int32_t* body_leaf, const double* x, const double* y, const double* z, const double* m,
+                      float4* loc, float soft2, double* ax, double* ay, double* az, double* pot);
 
 // p2p.cu
 __global__ void k_p2p_f64(DirList L, int ncells, CellsView cv, const double* x, const double* y, const double* z,

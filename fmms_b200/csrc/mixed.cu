@@ -477,22 +477,76 @@ __device__ __forceinline__ int unit_cell(const uint32_t* __restrict__ uoff, int 
     return lo;
 }
 
+// Body coordinates relative to their own leaf's centre, FP32, with the mass:
+// computed once per evaluation (the FP64 subtraction), so that staging a
+// source body for the near field is one 16-byte load plus its leaf's offset
+// from the target leaf's centre (c_s - c_t, FP64 rounded to FP32 once per
+// source leaf). The difference d = x_j - x_i then carries three FP32
+// roundings of quantities no larger than the pair's leaf separation instead
+// of one: the same order of absolute error.
+__global__ void k_local_coords(size_t n, const int32_t* __restrict__ body_leaf, CellsView cv,
+                               const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ z, const double* __restrict__ m,
+                               float4* __restrict__ loc) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int c = body_leaf[k];
+        loc[k] = make_float4((float)(x[k] - cv.cx[c]), (float)(y[k] - cv.cy[c]), (float)(z[k] - cv.cz[c]),
+                             (float)m[k]);
+    }
+}
+
+// One pair of source bodies (j, j+1) against one target, on packed FP32x2
+// arithmetic (sm_100's two-wide FP32 instructions: one issue slot for two
+// lanes of work): -x is the target's coordinate negated in both halves.
+// The pair's two partial sums stay apart in the two halves of each
+// accumulator until the tile ends.
+__device__ __forceinline__ void p2p_pair(const float4 a, const float4 b, float2 nx, float2 ny, float2 nz,
+                                         float2 soft2, float2& ax, float2& ay, float2& az, float2& pt) {
+    const float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx);
+    const float2 dy = __fadd2_rn(make_float2(a.z, a.w), ny);
+    const float2 dz = __fadd2_rn(make_float2(b.x, b.y), nz);
+    float2 r2 = __ffma2_rn(dz, dz, soft2);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    const float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    const float2 mi = __fmul2_rn(make_float2(b.z, b.w), inv);
+    const float2 f = __fmul2_rn(mi, __fmul2_rn(inv, inv));
+    ax = __ffma2_rn(f, dx, ax);
+    ay = __ffma2_rn(f, dy, ay);
+    az = __ffma2_rn(f, dz, az);
+    pt = __fadd2_rn(pt, mi);
+}
+
+// The pair with the target's own body at half h (0 or 1) of it: that half
+// becomes a massless body one unit away (no term).
+__device__ __forceinline__ void mask_self(float4& a, float4& b, int h, float x, float y, float z) {
+    if (h == 0) {
+        a.x = x + 1.f; a.z = y; b.x = z; b.z = 0.f;
+    } else {
+        a.y = x + 1.f; a.w = y; b.y = z; b.w = 0.f;
+    }
+}
+
 // TILE: source bodies staged per shared-memory tile (the tile shape the
-// autotuner picks). Each thread carries two targets, so every staged source
-// feeds two interactions; groups of G threads cover the leaf's targets and
-// R = BLOCK / G groups split each tile. The target's own slot is skipped by
-// position only in the tiles that overlap the target leaf itself. Blocks are
+// autotuner picks), as pairs: ta[q] = (x_2q, x_2q+1, y_2q, y_2q+1),
+// tz[q] = (z_2q, z_2q+1, m_2q, m_2q+1), an odd tile padded with a massless
+// body far away. Each thread carries two targets, so every staged pair feeds
+// four interactions; groups of G threads cover the leaf's targets and
+// R = BLOCK / G groups split each tile's pairs. The target's own body is
+// masked only in the tiles that overlap the target leaf itself. Blocks are
 // persistent and take units from a counter.
 template <int P2PM_TILE>
 __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv, P2pUnits U,
-                                                         const double* __restrict__ x, const double* __restrict__ y,
-                                                         const double* __restrict__ z, const double* __restrict__ m,
-                                                         float soft2, double* __restrict__ ax,
-                                                         double* __restrict__ ay, double* __restrict__ az,
-                                                         double* __restrict__ pot) {
-    __shared__ float4 tb[P2PM_TILE];  // x, y, z relative to the target centre; mass
+                                                         const float4* __restrict__ loc, float soft2_1,
+                                                         double* __restrict__ ax, double* __restrict__ ay,
+                                                         double* __restrict__ az, double* __restrict__ pot) {
+    constexpr int NPAIR = P2PM_TILE / 2;
+    constexpr int PPT = (NPAIR + P2PM_BLOCK - 1) / P2PM_BLOCK;  // pairs staged per thread
+    __shared__ float4 ta[NPAIR];
+    __shared__ float4 tz[NPAIR];
     __shared__ uint32_t pre[P2PM_SRC_CHUNK + 1];
     __shared__ uint32_t sfirst[P2PM_SRC_CHUNK];
+    __shared__ float4 soff[P2PM_SRC_CHUNK];  // source leaf centre - target leaf centre
     __shared__ uint32_t wsum[P2PM_BLOCK / 32];
     __shared__ int self_pos;
     __shared__ uint32_t unit_sh;
@@ -500,6 +554,7 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
     const int tid = threadIdx.x;
     const int lane = tid & 31, wid = tid >> 5;
     const uint32_t nunits = U.uoff[ncells];
+    const float2 soft2 = make_float2(soft2_1, soft2_1);
     for (;;) {
         if (tid == 0) unit_sh = atomicAdd(U.next, 1u);
         __syncthreads();
@@ -522,15 +577,15 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
             const bool has1 = active && i1 < nt;
             float x0 = 0, y0 = 0, z0 = 0, x1 = 0, y1 = 0, z1 = 0;
             if (active) {
-                x0 = (float)(x[tf + t0 + i0] - cx);
-                y0 = (float)(y[tf + t0 + i0] - cy);
-                z0 = (float)(z[tf + t0 + i0] - cz);
+                const float4 v = loc[tf + t0 + i0];
+                x0 = v.x; y0 = v.y; z0 = v.z;
             }
             if (has1) {
-                x1 = (float)(x[tf + t0 + i1] - cx);
-                y1 = (float)(y[tf + t0 + i1] - cy);
-                z1 = (float)(z[tf + t0 + i1] - cz);
+                const float4 v = loc[tf + t0 + i1];
+                x1 = v.x; y1 = v.y; z1 = v.z;
             }
+            const float2 nx0 = make_float2(-x0, -x0), ny0 = make_float2(-y0, -y0), nz0 = make_float2(-z0, -z0);
+            const float2 nx1 = make_float2(-x1, -x1), ny1 = make_float2(-y1, -y1), nz1 = make_float2(-z1, -z1);
             DS a0x{0, 0}, a0y{0, 0}, a0z{0, 0}, p0{0, 0}, a1x{0, 0}, a1y{0, 0}, a1z{0, 0}, p1{0, 0};
             for (uint32_t sc = beg; sc < end; sc += P2PM_SRC_CHUNK) {
                 const int ns = (int)min((uint32_t)P2PM_SRC_CHUNK, end - sc);
@@ -540,10 +595,13 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                 for (int q0 = 0; q0 < ns; q0 += P2PM_BLOCK) {
                     const int q = q0 + tid;
                     uint32_t v = 0;
+                    int src = -1;
                     if (q < ns) {
-                        const int src = (int)L.src(L.key(sc + q));
+                        src = (int)L.src(L.key(sc + q));
                         v = cv.count[src];
                         sfirst[q] = cv.first[src];
+                        soff[q] = make_float4((float)(cv.cx[src] - cx), (float)(cv.cy[src] - cy),
+                                              (float)(cv.cz[src] - cz), 0.f);
                     }
                     uint32_t incl = v;
                     for (int o = 1; o < 32; o <<= 1) {
@@ -556,7 +614,7 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                     for (int w = 0; w < wid; ++w) base += wsum[w];
                     if (q < ns) {
                         pre[q + 1] = base + incl;
-                        if ((int)L.src(L.key(sc + q)) == c) self_pos = (int)(base + incl - v);
+                        if (src == c) self_pos = (int)(base + incl - v);
                     }
                     if (q0 == 0 && tid == 0) pre[0] = 0;
                     __syncthreads();
@@ -565,49 +623,69 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                 const int sp = self_pos;  // position of the target leaf in this chunk's sources, or -1
                 for (uint32_t b0 = 0; b0 < total; b0 += P2PM_TILE) {
                     const uint32_t nb = min((uint32_t)P2PM_TILE, total - b0);
-                    for (uint32_t t = tid; t < nb; t += P2PM_BLOCK) {
-                        const uint32_t gg = b0 + t;
+                    const int npair = (int)(nb + 1) >> 1;
+                    // stage PPT consecutive pairs per thread: one search for the
+                    // first body's leaf, then step leaf by leaf
+                    if (tid * PPT < npair) {
+                        uint32_t gg = b0 + 2u * (uint32_t)(tid * PPT);
                         int lo = 0, hi = ns;
                         while (hi - lo > 1) {
                             const int mid = (lo + hi) >> 1;
                             if (pre[mid] <= gg) lo = mid;
                             else hi = mid;
                         }
-                        const uint32_t slot = sfirst[lo] + (gg - pre[lo]);
-                        tb[t] = make_float4((float)(x[slot] - cx), (float)(y[slot] - cy), (float)(z[slot] - cz),
-                                            (float)m[slot]);
+#pragma unroll
+                        for (int e = 0; e < PPT; ++e) {
+                            const int q = tid * PPT + e;
+                            if (q < npair) {
+                                float4 s2[2];
+#pragma unroll
+                                for (int h = 0; h < 2; ++h, ++gg) {
+                                    if (gg < b0 + nb) {
+                                        while (gg >= pre[lo + 1]) ++lo;
+                                        const float4 v = loc[sfirst[lo] + (gg - pre[lo])];
+                                        const float4 o = soff[lo];
+                                        s2[h] = make_float4(v.x + o.x, v.y + o.y, v.z + o.z, v.w);
+                                    } else {
+                                        s2[h] = make_float4(1e18f, 0.f, 0.f, 0.f);  // massless padding
+                                    }
+                                }
+                                ta[q] = make_float4(s2[0].x, s2[1].x, s2[0].y, s2[1].y);
+                                tz[q] = make_float4(s2[0].z, s2[1].z, s2[0].w, s2[1].w);
+                            }
+                        }
                     }
                     __syncthreads();
                     if (active) {
-                        float q0x = 0, q0y = 0, q0z = 0, q0p = 0, q1x = 0, q1y = 0, q1z = 0, q1p = 0;
+                        float2 q0x{0, 0}, q0y{0, 0}, q0z{0, 0}, q0p{0, 0}, q1x{0, 0}, q1y{0, 0}, q1z{0, 0}, q1p{0, 0};
                         const bool overlaps = sp >= 0 && (uint32_t)sp < b0 + nb && (uint32_t)sp + tn > b0;
                         if (!overlaps) {
-#pragma unroll 4
-                            for (uint32_t j = rep; j < nb; j += R) {
-                                const float4 sj = tb[j];
-                                p2p_term(sj, x0, y0, z0, soft2, q0x, q0y, q0z, q0p);
-                                p2p_term(sj, x1, y1, z1, soft2, q1x, q1y, q1z, q1p);
+#pragma unroll 2
+                            for (int j = rep; j < npair; j += R) {
+                                const float4 a = ta[j], b = tz[j];
+                                p2p_pair(a, b, nx0, ny0, nz0, soft2, q0x, q0y, q0z, q0p);
+                                p2p_pair(a, b, nx1, ny1, nz1, soft2, q1x, q1y, q1z, q1p);
                             }
                         } else {
                             // the target's own body sits at position sp + t0 + i in the sources
                             const int s0 = sp + (int)t0 + i0 - (int)b0, s1 = sp + (int)t0 + i1 - (int)b0;
-                            for (uint32_t j = rep; j < nb; j += R) {
-                                float4 sj = tb[j];
-                                float4 sa = sj, sb = sj;
-                                if ((int)j == s0) sa = make_float4(x0 + 1.f, y0, z0, 0.f);  // no term
-                                if ((int)j == s1) sb = make_float4(x1 + 1.f, y1, z1, 0.f);
-                                p2p_term(sa, x0, y0, z0, soft2, q0x, q0y, q0z, q0p);
-                                p2p_term(sb, x1, y1, z1, soft2, q1x, q1y, q1z, q1p);
+                            for (int j = rep; j < npair; j += R) {
+                                const float4 a = ta[j], b = tz[j];
+                                float4 a0 = a, b0v = b, a1 = a, b1v = b;
+                                if (s0 >= 0 && j == (s0 >> 1)) mask_self(a0, b0v, s0 & 1, x0, y0, z0);
+                                if (s1 >= 0 && j == (s1 >> 1)) mask_self(a1, b1v, s1 & 1, x1, y1, z1);
+                                p2p_pair(a0, b0v, nx0, ny0, nz0, soft2, q0x, q0y, q0z, q0p);
+                                p2p_pair(a1, b1v, nx1, ny1, nz1, soft2, q1x, q1y, q1z, q1p);
                             }
                         }
-                        ds_add(a0x, q0x);
-                        ds_add(a0y, q0y);
-                        ds_add(a0z, q0z);
-                        ds_add(p0, q0p);
-                        ds_add(a1x, q1x);
-                        ds_add(a1y, q1y);
-                        ds_add(a1z, q1z);
-                        ds_add(p1, q1p);
+                        ds_add(a0x, q0x.x + q0x.y);
+                        ds_add(a0y, q0y.x + q0y.y);
+                        ds_add(a0z, q0z.x + q0z.y);
+                        ds_add(p0, q0p.x + q0p.y);
+                        ds_add(a1x, q1x.x + q1x.y);
+                        ds_add(a1y, q1y.x + q1y.y);
+                        ds_add(a1z, q1z.x + q1z.y);
+                        ds_add(p1, q1p.x + q1p.y);
                     }
                     __syncthreads();
                 }
@@ -674,22 +752,22 @@ void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const
 }
 
 template <int TILE>
-static void launch_tile(int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, const double* x,
-                        const double* y, const double* z, const double* m, float soft2, double* ax, double* ay,
-                        double* az, double* pot) {
+static void launch_tile(int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, const float4* loc,
+                        float soft2, double* ax, double* ay, double* az, double* pot) {
     int per_sm = 0;  // persistent blocks: as many as fit on an SM at once
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2p_mixed<TILE>, P2PM_BLOCK, 0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    k_p2p_mixed<TILE><<<nsm * per_sm, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+    k_p2p_mixed<TILE><<<nsm * per_sm, P2PM_BLOCK, 0, s>>>(L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
 }
 
-void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U,
-                      const double* x, const double* y, const double* z, const double* m, float soft2, double* ax,
-                      double* ay, double* az, double* pot) {
-    if (tile <= 128) launch_tile<128>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
-    else if (tile <= 256) launch_tile<256>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
-    else launch_tile<512>(nsm, s, L, ncells, cv, U, x, y, z, m, soft2, ax, ay, az, pot);
+void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, size_t n,
+                      const int32_t* body_leaf, const double* x, const double* y, const double* z, const double* m,
+                      float4* loc, float soft2, double* ax, double* ay, double* az, double* pot) {
+    k_local_coords<<<grid_for(n, 256), 256, 0, s>>>(n, body_leaf, cv, x, y, z, m, loc);
+    if (tile <= 128) launch_tile<128>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
+    else if (tile <= 256) launch_tile<256>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
+    else launch_tile<512>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
     k_p2p_combine<<<grid_for((size_t)ncells * 32, 256), 256, 0, s>>>(ncells, cv, U, ax, ay, az, pot);
 }
 

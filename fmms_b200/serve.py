@@ -33,16 +33,23 @@ predicted with it -- the batch's last measured step latency plus the session's
 calibrated extra latency (the larger of the two system types) -- stays within
 `headroom` times the isolated latency (the smaller of the two types) of the
 batch's smallest session, and only while the lane's recent steps stay within
-that bound (feedback against prediction error). The joining tick measures the
-prediction: its ratio to the prediction (kept >= 1, decaying) scales later
-predictions, and if it took longer than `headroom` times the isolated latency of the
-batch's smallest session, the sessions that joined in it (all of them when
-others were already stepping, else all but the first) -- which have not
-stepped yet, so nothing of theirs changes -- go back to the front of the queue
-and wait for a session of the lane to finish before they are tried again. The queue is scanned in arrival
+that bound (feedback against prediction error). A tick in which sessions join
+a running batch is a step interval of the sessions already stepping, so it
+measures the prediction: its ratio to the prediction (kept >= 1, decaying as
+sessions finish) scales later predictions, and if it took longer than
+`headroom` times the isolated latency of the batch's smallest session, the
+sessions that joined in it -- which have not stepped yet, so nothing of theirs
+changes -- go back to the front of the queue and wait for a session of the
+lane to finish before they are tried again. Sessions that start together in an
+empty lane are bounded by the model alone (their joining tick, with the
+one-time costs of joining, is no session's step). Only the first session of an
+empty lane may join before the background copies have put its bodies on the
+device. The queue is scanned in arrival
 order and sessions that fit may overtake ones that do not, except a session
-that has waited longer than `max_bypass_s`: nobody overtakes it. Waiting time
-is reported apart from the step latency.
+that has waited longer than `max_bypass_s`: nobody overtakes it, save the
+sessions that start together with an older one in an empty lane (their steps
+end with that session's, so they keep the waiting one out no longer). Waiting
+time is reported apart from the step latency.
 
 By default there is one lane. Several lanes (`lanes`: lower bounds of N) run
 concurrently on streams of decreasing priority for increasing N; they share
@@ -102,6 +109,7 @@ class Session:
     staged: tuple | None = dataclasses.field(default=None, repr=False)  # device pos, vel, mass, ready event
     pending: tuple | None = dataclasses.field(default=None, repr=False)  # result copy job, host pos, host vel
     stage_job: object | None = dataclasses.field(default=None, repr=False)  # staging in progress
+    planned: bool = False  # counted in the staging budget (queued for staging, staging, or staged)
 
     @property
     def n(self) -> int:
@@ -114,7 +122,7 @@ class Session:
         """The same request, not yet served."""
         return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
                                    primed=False, last_end=0.0, retry_after=-1, step_ms=[], result_pos=None,
-                                   result_vel=None, staged=None, pending=None, stage_job=None)
+                                   result_vel=None, staged=None, pending=None, stage_job=None, planned=False)
 
 
 def _interp_loglog(ns, vals, n):
@@ -313,9 +321,15 @@ class Lane:
         # predicted step latency of the batch as it stands, and its smallest member
         tau = self.predicted_ms if self.predicted_ms is not None else self.last_interval_ms
         nmin = min((s.n for s in self.members), default=None)
+        was_empty = not self.members
         for s in list(self.queue)[: srv.scan]:
             pred = None
             fits = s.retry_after < self.departures
+            if fits and (new or self.members) and s.staged is None:
+                # only the first session of an empty lane joins before its
+                # bodies are on the device: a copy inside a tick would stretch
+                # every member's step
+                fits = False
             if fits and model is not None and nmin is not None:
                 pred = (tau if tau is not None else model.iso(nmin)) + model.extra(s.n)
                 fits = pred * self.corr <= srv.headroom * model.iso(min(nmin, s.n))
@@ -328,6 +342,12 @@ class Lane:
                 nmin = s.n if nmin is None else min(nmin, s.n)
                 continue
             if model is None or (s.submitted_at is not None and now - s.submitted_at > srv.max_bypass_s):
+                if model is not None and was_empty and new:
+                    # the lane was empty and the oldest session has just been
+                    # admitted: sessions that fit beside it start with it (the
+                    # batch ends no later for them), and the one that does not
+                    # fit heads the next batch
+                    continue
                 break  # first come, first served from this session on
         if new and model is not None:
             self.predicted_ms = tau
@@ -383,6 +403,7 @@ class Lane:
         for s in reversed(sessions):
             s.admitted_at = None
             s.retry_after = self.departures
+            s.planned = False  # its device copy went into the lane's rows: staged again before a retry
             self.srv.release(s.bytes_needed())
             self.queue.appendleft(s)
         self.evictions += len(sessions)
@@ -403,6 +424,8 @@ class Lane:
                 keep.append(s)
                 rows.append(torch.arange(a, b, device=self.srv.dev))
         self.departures += len(out)
+        for _ in out:  # the learned under-prediction of joins fades as sessions finish
+            self.corr = max(1.0, 0.9 * self.corr)
         for s, p, v in out:
             ev = torch.cuda.Event()
             ev.record(self.stream)
@@ -479,13 +502,18 @@ class Lane:
                     self.recent_ratio.append(max(s.step_ms[-1] / self.srv.model.iso(s.n) for s in stepping))
             joined = [s for s in self.members if not s.primed]
             model = self.srv.model
-            if joined and model is not None and len(self.members) > 1:
-                # learn how far the model under-predicts joins (decaying toward 1)
+            if joined and model is not None and stepping:
+                # a join into a running batch: this tick is a step interval of
+                # the sessions already stepping. Learn how far the model
+                # under-predicts joins (decaying toward 1), and undo the join
+                # if the tick broke the bound. (A batch started in an empty
+                # lane is bounded by the model alone: its joining tick, with
+                # the one-time costs of joining, is no session's step.)
                 if predicted:
                     seen = 1e3 * (t_end - t_start) / predicted
                     self.corr = min(4.0, max(1.0, 0.9 * self.corr, seen))
                 ratio = 1e3 * (t_end - t_start) / model.iso(min(s.n for s in self.members))
-                undo = joined if stepping else joined[1:]
+                undo = joined
                 if ratio > self.srv.headroom and undo:
                     self.evict(undo)
                     joined = [s for s in joined if s not in undo]
@@ -675,14 +703,27 @@ class Server:
                 self.to_stage.remove(s)
             else:
                 self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+                s.planned = True
         if s.stage_job is None:
             self._start_staging(s)
         self.ring.finish(s.stage_job[0], self.copy_stream)
         self._end_staging(s)
 
     def unstage(self, n_bodies):
+        """Give back staging budget, and plan the staging of queued sessions
+        that did not fit in it when they were submitted (in queue order)."""
         with self.lock:
             self.staged_bytes -= n_bodies * STAGED_BYTES_PER_BODY
+            for ln in self.lanes:
+                for s in list(ln.queue)[: self.scan]:
+                    if s.planned:
+                        continue
+                    nb = s.n * STAGED_BYTES_PER_BODY
+                    if self.staged_bytes + nb > self.stage_limit:
+                        break
+                    self.staged_bytes += nb
+                    s.planned = True
+                    self.to_stage.append(s)
 
     def pump(self, budget_s: float) -> bool:
         """Result copies first, then staging, one chunk at a time, for about
@@ -774,6 +815,7 @@ class Server:
         with self.lock:
             if self.staged_bytes + s.n * STAGED_BYTES_PER_BODY <= self.stage_limit:
                 self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
+                s.planned = True
                 self.to_stage.append(s)
             self.outstanding += 1
             (lane or self.lane_for(s)).queue.append(s)

@@ -14,9 +14,12 @@ import pytest
 from fmms_b200.serve import TICK_FIELDS, Lane, LatencyModel, Session, worst_intervals
 
 
-def session(sid, n, submitted_at=0.0):
+def session(sid, n, submitted_at=0.0, staged=True):
     s = Session(sid=sid, mass=np.zeros(n), pos=np.zeros((n, 3)), vel=np.zeros((n, 3)), steps=10, dt=1e-3)
     s.submitted_at = submitted_at
+    if staged:  # bodies already copied to the device (a stand-in for the tensors and event)
+        s.staged = (None, None, None, None)
+        s.planned = True
     return s
 
 
@@ -63,10 +66,54 @@ def test_admission_latency_bound_and_overtaking():
 
 
 def test_admission_no_overtaking_past_a_long_wait():
+    member = session(9, 1000)
+    small1, big, small2 = session(0, 1000), session(1, 1_000_000, submitted_at=0.0), session(2, 1000)
+    ln = fake_lane([small1, big, small2], members=[member], max_bypass_s=2.0)
+    ln.last_interval_ms = 1.01
+    new = Lane.admit(ln, now=5.0)  # big has waited 5 s > 2 s: nobody passes it while the lane runs
+    assert new == [small1] and list(ln.queue) == [big, small2]
+
+
+def test_admission_fresh_batch_takes_sessions_that_fit_past_a_long_wait():
+    """In an empty lane the oldest session starts a batch; sessions that fit
+    beside it start with it even past one that has waited long, which heads
+    the next batch (their steps end together, so it waits no longer)."""
     small1, big, small2 = session(0, 1000), session(1, 1_000_000, submitted_at=0.0), session(2, 1000)
     ln = fake_lane([small1, big, small2], max_bypass_s=2.0)
-    new = Lane.admit(ln, now=5.0)  # big has waited 5 s > 2 s: nobody passes it
-    assert new == [small1] and list(ln.queue) == [big, small2]
+    assert Lane.admit(ln, now=5.0) == [small1, small2]
+    assert list(ln.queue) == [big]
+    ln2 = fake_lane([big, small1, small2], max_bypass_s=2.0)
+    assert Lane.admit(ln2, now=5.0) == [big]  # 10.01 + 0.01 > 1.6 * iso(1000)
+    assert list(ln2.queue) == [small1, small2]
+
+
+def test_admission_followers_must_be_staged():
+    """Only the first session of an empty lane may join before its bodies
+    are on the device; an unstaged one is passed over, not waited for."""
+    head, cold, warm = session(0, 1000, staged=False), session(1, 1000, staged=False), session(2, 1000)
+    ln = fake_lane([head, cold, warm])
+    assert Lane.admit(ln, now=1.0) == [head, warm]
+    assert list(ln.queue) == [cold]
+    member = session(9, 1000)
+    ln2 = fake_lane([session(3, 1000, staged=False)], members=[member])
+    ln2.last_interval_ms = 1.01
+    assert Lane.admit(ln2, now=1.0) == []
+
+
+def test_unstage_plans_queued_sessions_in_order():
+    """Staging budget given back goes to queued sessions that did not fit in
+    it when they were submitted, in queue order, up to the limit."""
+    import threading
+
+    from fmms_b200.serve import STAGED_BYTES_PER_BODY, Server
+
+    a, b, c = session(0, 1000, staged=False), session(1, 2000, staged=False), session(2, 500, staged=False)
+    lane = SimpleNamespace(queue=deque([a, b, c]))
+    srv = SimpleNamespace(lock=threading.Lock(), lanes=[lane], scan=256, to_stage=deque(),
+                          stage_limit=2500 * STAGED_BYTES_PER_BODY, staged_bytes=2000 * STAGED_BYTES_PER_BODY)
+    Server.unstage(srv, 1000)  # 1000 bodies' worth left in use, room for 1500 more
+    assert list(srv.to_stage) == [a] and a.planned and not b.planned and not c.planned
+    assert srv.staged_bytes == 2000 * STAGED_BYTES_PER_BODY
 
 
 def test_admission_hbm_reservation_and_gate():
