@@ -28,7 +28,7 @@ def _forest(parts):
 
 def tune_ensemble(parts, *, p=8, theta=0.5, softening=1e-3, precision="mixed", device=0, err_target=1e-5,
                   margin=0.6, thetas=(0.5, 0.4), gaps=(0.0, 100.0, 200.0, 400.0), orders=None,
-                  leaves=(32, 48, 64, 96, 128), tiles=(128, 256), sample_every=8, repeats=2, finalists=3):
+                  leaves=(32, 48, 64, 96, 128), tiles=(256, 512), sample_every=8, repeats=2, finalists=3):
     import torch
 
     import fmms_b200 as fx
@@ -72,14 +72,14 @@ def tune_ensemble(parts, *, p=8, theta=0.5, softening=1e-3, precision="mixed", d
                 "err_p99_worst": worst}
 
     bound = margin * err_target
-    cands = [run(th, gap, pp, 64, 256) for th in thetas for gap in gaps for pp in orders]
+    cands = [run(th, gap, pp, 64, 512) for th in thetas for gap in gaps for pp in orders]
     accurate = sorted((c for c in cands if c["err_p99_worst"] <= bound), key=lambda c: c["ms"])
     if not accurate:  # nothing meets the bound: the most accurate settings
         accurate = sorted(cands, key=lambda c: c["err_p99_worst"])
     for c0 in accurate[:finalists]:
         for nl in leaves:
             for tile in tiles:
-                if (nl, tile) != (64, 256):
+                if (nl, tile) != (64, 512):
                     cands.append(run(c0["theta"], c0["soft_gap"], c0["p"], nl, tile))
     ok = [c for c in cands if c["err_p99_worst"] <= bound]
     if ok:

@@ -779,7 +779,7 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
     CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
     const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_soff.p, ctx->p2p_part.p, ctx->p2p_next.p};
-    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 256, ctx->nsm, s2, lp, nc, cv, units, n,
+    launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 512, ctx->nsm, s2, lp, nc, cv, units, n,
                      ctx->body_leaf.p, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, ctx->body_loc.p, soft2, ctx->nax.p,
                      ctx->nay.p, ctx->naz.p, ctx->npot.p);
     CKL("p2p (mixed)");

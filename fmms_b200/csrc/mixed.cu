@@ -400,8 +400,9 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* __restrict__ body_leaf, con
 // FP32 P2P with compensated accumulation. Source bodies are staged in shared
 // memory relative to the target leaf's centre (the FP64 subtraction), so the
 // FP32 differences d = x_j - x_i keep their relative precision; each thread
-// sums a tile in FP32 and adds the tile's partial into a double-single
-// (hi, lo) accumulator with an error-free TwoSum. 1/r by the hardware rsqrt.
+// sums at least P2PM_FLUSH source pairs (two partial sums per component) in
+// FP32 and adds them into a double-single (hi, lo) accumulator with an
+// error-free TwoSum. 1/r by the hardware rsqrt.
 #define P2PM_BLOCK 128
 #define P2PM_SRC_CHUNK 256
 
@@ -535,8 +536,77 @@ __device__ __forceinline__ void mask_self(float4& a, float4& b, int h, float x, 
 // R = BLOCK / G groups split each tile's pairs. The target's own body is
 // masked only in the tiles that overlap the target leaf itself. Blocks are
 // persistent and take units from a counter.
+//
+// The sources are taken in chunks of at most P2PM_SRC_CHUNK source leaves and
+// P2PM_MAP bodies: a chunk's bodies are numbered consecutively and own[]
+// gives each body's leaf in the chunk, so staging a body is a table lookup
+// (a leaf of more than P2PM_MAP bodies is a chunk of its own, without the
+// table). A target chunk's sums over the R groups are reduced by all threads,
+// S threads per output in fixed strips and a fixed shuffle tree.
+#define P2PM_MAP 4096
+#define P2PM_FLUSH 16
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Start copying the bodies of the tile [b0, b0 + nb) of a chunk to raw[]:
+// thread tid takes pairs tid, tid + BLOCK, ...; lq[] keeps each body's leaf
+// in the chunk (-1: padding past the tile's end).
+template <int PPT>
+__device__ __forceinline__ void stage_issue(uint32_t b0, uint32_t nb, int tid, bool mapped,
+                                            const uint8_t* own, const uint32_t* sbase,
+                                            const float4* __restrict__ loc, float4* raw, int* lq) {
+    const int npair = (int)(nb + 1) >> 1;
+#pragma unroll
+    for (int e = 0; e < PPT; ++e) {
+        const int q = tid + e * P2PM_BLOCK;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t gg = b0 + 2u * (uint32_t)q + (uint32_t)h;
+            lq[2 * e + h] = -1;
+            if (q < npair && gg < b0 + nb) {
+                const int l = mapped ? (int)own[gg] : 0;
+                lq[2 * e + h] = l;
+                cp_async16(raw + 2 * q + h, loc + (gg + sbase[l]));
+            }
+        }
+    }
+    cp_async_commit();
+}
+
+// Finish the bodies this thread copied: wait for its copies, add the leaf
+// offsets and write the pair layout.
+template <int PPT>
+__device__ __forceinline__ void stage_finish(int npair, int tid, const float4* raw, const float4* soff,
+                                             const int* lq, float4* ta, float4* tz) {
+    cp_async_wait_all();
+#pragma unroll
+    for (int e = 0; e < PPT; ++e) {
+        const int q = tid + e * P2PM_BLOCK;
+        if (q < npair) {
+            float4 s2[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int l = lq[2 * e + h];
+                if (l >= 0) {
+                    const float4 v = raw[2 * q + h];
+                    const float4 o = soff[l];
+                    s2[h] = make_float4(v.x + o.x, v.y + o.y, v.z + o.z, v.w);
+                } else {
+                    s2[h] = make_float4(1e18f, 0.f, 0.f, 0.f);  // massless padding
+                }
+            }
+            ta[q] = make_float4(s2[0].x, s2[1].x, s2[0].y, s2[1].y);
+            tz[q] = make_float4(s2[0].z, s2[1].z, s2[0].w, s2[1].w);
+        }
+    }
+}
 template <int P2PM_TILE>
-__global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells, CellsView cv, P2pUnits U,
+__global__ void __launch_bounds__(P2PM_BLOCK, 5) k_p2p_mixed(DirList L, int ncells, CellsView cv, P2pUnits U,
                                                          const float4* __restrict__ loc, float soft2_1,
                                                          double* __restrict__ ax, double* __restrict__ ay,
                                                          double* __restrict__ az, double* __restrict__ pot) {
@@ -544,11 +614,13 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
     constexpr int PPT = (NPAIR + P2PM_BLOCK - 1) / P2PM_BLOCK;  // pairs staged per thread
     __shared__ float4 ta[NPAIR];
     __shared__ float4 tz[NPAIR];
+    __shared__ float4 raw[P2PM_TILE];  // the next tile's bodies as copied (leaf-relative)
     __shared__ uint32_t pre[P2PM_SRC_CHUNK + 1];
-    __shared__ uint32_t sfirst[P2PM_SRC_CHUNK];
-    __shared__ float4 soff[P2PM_SRC_CHUNK];  // source leaf centre - target leaf centre
+    __shared__ uint32_t sbase[P2PM_SRC_CHUNK];  // first slot of the leaf - its first position in the chunk
+    __shared__ float4 soff[P2PM_SRC_CHUNK];     // source leaf centre - target leaf centre
+    __shared__ uint8_t own[P2PM_MAP];
     __shared__ uint32_t wsum[P2PM_BLOCK / 32];
-    __shared__ int self_pos;
+    __shared__ int self_pos, nuse_sh;
     __shared__ uint32_t unit_sh;
     __shared__ float red[16][P2PM_BLOCK];
     const int tid = threadIdx.x;
@@ -587,21 +659,38 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
             const float2 nx0 = make_float2(-x0, -x0), ny0 = make_float2(-y0, -y0), nz0 = make_float2(-z0, -z0);
             const float2 nx1 = make_float2(-x1, -x1), ny1 = make_float2(-y1, -y1), nz1 = make_float2(-z1, -z1);
             DS a0x{0, 0}, a0y{0, 0}, a0z{0, 0}, p0{0, 0}, a1x{0, 0}, a1y{0, 0}, a1z{0, 0}, p1{0, 0};
-            for (uint32_t sc = beg; sc < end; sc += P2PM_SRC_CHUNK) {
+            // FP32 partial sums, added into the double-single sums once they
+            // hold P2PM_FLUSH source pairs (and at the end)
+            float2 q0x{0, 0}, q0y{0, 0}, q0z{0, 0}, q0p{0, 0}, q1x{0, 0}, q1y{0, 0}, q1z{0, 0}, q1p{0, 0};
+            int held = 0;
+            auto flush = [&]() {
+                ds_add(a0x, q0x.x + q0x.y);
+                ds_add(a0y, q0y.x + q0y.y);
+                ds_add(a0z, q0z.x + q0z.y);
+                ds_add(p0, q0p.x + q0p.y);
+                ds_add(a1x, q1x.x + q1x.y);
+                ds_add(a1y, q1y.x + q1y.y);
+                ds_add(a1z, q1z.x + q1z.y);
+                ds_add(p1, q1p.x + q1p.y);
+                q0x = q0y = q0z = q0p = q1x = q1y = q1z = q1p = make_float2(0.f, 0.f);
+                held = 0;
+            };
+            for (uint32_t sc = beg; sc < end;) {
                 const int ns = (int)min((uint32_t)P2PM_SRC_CHUNK, end - sc);
                 __syncthreads();
                 if (tid == 0) self_pos = -1;
                 // exclusive prefix of source leaf sizes (warp scans, then warp totals)
-                for (int q0 = 0; q0 < ns; q0 += P2PM_BLOCK) {
+                int myq[2] = {-1, -1};
+                for (int q0 = 0, h = 0; q0 < ns; q0 += P2PM_BLOCK, ++h) {
                     const int q = q0 + tid;
                     uint32_t v = 0;
                     int src = -1;
                     if (q < ns) {
                         src = (int)L.src(L.key(sc + q));
                         v = cv.count[src];
-                        sfirst[q] = cv.first[src];
                         soff[q] = make_float4((float)(cv.cx[src] - cx), (float)(cv.cy[src] - cy),
                                               (float)(cv.cz[src] - cz), 0.f);
+                        myq[h] = src;
                     }
                     uint32_t incl = v;
                     for (int o = 1; o < 32; o <<= 1) {
@@ -614,50 +703,47 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                     for (int w = 0; w < wid; ++w) base += wsum[w];
                     if (q < ns) {
                         pre[q + 1] = base + incl;
-                        if (src == c) self_pos = (int)(base + incl - v);
+                        sbase[q] = cv.first[src] - (base + incl - v);
                     }
                     if (q0 == 0 && tid == 0) pre[0] = 0;
                     __syncthreads();
                 }
-                const uint32_t total = pre[ns];
+                // the leaves whose bodies fit in the table (at least one)
+                int fit = 0;
+                for (int q = tid; q < ns; q += P2PM_BLOCK) fit += pre[q + 1] <= P2PM_MAP ? 1 : 0;
+                if (tid == 0) nuse_sh = 0;
+                __syncthreads();
+                if (fit) atomicAdd(&nuse_sh, fit);
+                __syncthreads();
+                const int nl = max(1, nuse_sh);
+                const bool mapped = pre[nl] <= P2PM_MAP;
+                for (int h = 0; h < 2; ++h) {
+                    const int q = tid + h * P2PM_BLOCK;
+                    if (q < nl) {
+                        if (myq[h] == c) self_pos = (int)pre[q];
+                        if (mapped)
+                            for (uint32_t e = pre[q]; e < pre[q + 1]; ++e) own[e] = (uint8_t)q;
+                    }
+                }
+                __syncthreads();
+                const uint32_t total = pre[nl];
                 const int sp = self_pos;  // position of the target leaf in this chunk's sources, or -1
+                sc += nl;
+                // tile k + 1's bodies are copied to raw[] (cp.async) while tile k
+                // is computed; each thread later finishes the bodies it copied
+                // (its leaf's offset added, pair layout), so only the tile
+                // hand-over needs a block barrier
+                int lq_cur[2 * PPT], lq_nxt[2 * PPT];
+                stage_issue<PPT>(0, min((uint32_t)P2PM_TILE, total), tid, mapped, own, sbase, loc, raw, lq_cur);
                 for (uint32_t b0 = 0; b0 < total; b0 += P2PM_TILE) {
                     const uint32_t nb = min((uint32_t)P2PM_TILE, total - b0);
                     const int npair = (int)(nb + 1) >> 1;
-                    // stage PPT consecutive pairs per thread: one search for the
-                    // first body's leaf, then step leaf by leaf
-                    if (tid * PPT < npair) {
-                        uint32_t gg = b0 + 2u * (uint32_t)(tid * PPT);
-                        int lo = 0, hi = ns;
-                        while (hi - lo > 1) {
-                            const int mid = (lo + hi) >> 1;
-                            if (pre[mid] <= gg) lo = mid;
-                            else hi = mid;
-                        }
-#pragma unroll
-                        for (int e = 0; e < PPT; ++e) {
-                            const int q = tid * PPT + e;
-                            if (q < npair) {
-                                float4 s2[2];
-#pragma unroll
-                                for (int h = 0; h < 2; ++h, ++gg) {
-                                    if (gg < b0 + nb) {
-                                        while (gg >= pre[lo + 1]) ++lo;
-                                        const float4 v = loc[sfirst[lo] + (gg - pre[lo])];
-                                        const float4 o = soff[lo];
-                                        s2[h] = make_float4(v.x + o.x, v.y + o.y, v.z + o.z, v.w);
-                                    } else {
-                                        s2[h] = make_float4(1e18f, 0.f, 0.f, 0.f);  // massless padding
-                                    }
-                                }
-                                ta[q] = make_float4(s2[0].x, s2[1].x, s2[0].y, s2[1].y);
-                                tz[q] = make_float4(s2[0].z, s2[1].z, s2[0].w, s2[1].w);
-                            }
-                        }
-                    }
+                    stage_finish<PPT>(npair, tid, raw, soff, lq_cur, ta, tz);
                     __syncthreads();
+                    if (b0 + P2PM_TILE < total)
+                        stage_issue<PPT>(b0 + P2PM_TILE, min((uint32_t)P2PM_TILE, total - b0 - P2PM_TILE), tid,
+                                         mapped, own, sbase, loc, raw, lq_nxt);
                     if (active) {
-                        float2 q0x{0, 0}, q0y{0, 0}, q0z{0, 0}, q0p{0, 0}, q1x{0, 0}, q1y{0, 0}, q1z{0, 0}, q1p{0, 0};
                         const bool overlaps = sp >= 0 && (uint32_t)sp < b0 + nb && (uint32_t)sp + tn > b0;
                         if (!overlaps) {
 #pragma unroll 2
@@ -678,39 +764,46 @@ __global__ void __launch_bounds__(P2PM_BLOCK) k_p2p_mixed(DirList L, int ncells,
                                 p2p_pair(a1, b1v, nx1, ny1, nz1, soft2, q1x, q1y, q1z, q1p);
                             }
                         }
-                        ds_add(a0x, q0x.x + q0x.y);
-                        ds_add(a0y, q0y.x + q0y.y);
-                        ds_add(a0z, q0z.x + q0z.y);
-                        ds_add(p0, q0p.x + q0p.y);
-                        ds_add(a1x, q1x.x + q1x.y);
-                        ds_add(a1y, q1y.x + q1y.y);
-                        ds_add(a1z, q1z.x + q1z.y);
-                        ds_add(p1, q1p.x + q1p.y);
+                        held += (npair - rep + R - 1) / R;
+                        if (held >= P2PM_FLUSH) flush();
                     }
                     __syncthreads();
+#pragma unroll
+                    for (int e = 0; e < 2 * PPT; ++e) lq_cur[e] = lq_nxt[e];
                 }
             }
+            flush();
             red[0][tid] = a0x.hi; red[1][tid] = a0x.lo; red[2][tid] = a0y.hi; red[3][tid] = a0y.lo;
             red[4][tid] = a0z.hi; red[5][tid] = a0z.lo; red[6][tid] = p0.hi; red[7][tid] = p0.lo;
             red[8][tid] = a1x.hi; red[9][tid] = a1x.lo; red[10][tid] = a1y.hi; red[11][tid] = a1y.lo;
             red[12][tid] = a1z.hi; red[13][tid] = a1z.lo; red[14][tid] = p1.hi; red[15][tid] = p1.lo;
             __syncthreads();
-            if (tid < nt) {
-                const int gi = tid % G, half = tid / G;  // target tid = gi + half * G
-                double sacc[4] = {0, 0, 0, 0};
-                for (int r = 0; r < R; ++r) {
-                    const int q = r * G + gi;
-                    for (int k4 = 0; k4 < 4; ++k4)
-                        sacc[k4] += (double)red[8 * half + 2 * k4][q] + (double)red[8 * half + 2 * k4 + 1][q];
+            // outputs: nt targets x 4 components; S threads per output (a power
+            // of two up to 32, so an output's threads share a warp)
+            const int nout = 4 * nt;
+            int S = 1;
+            while (S < 32 && 2 * S * nout <= P2PM_BLOCK) S <<= 1;
+            for (int o0 = 0; o0 < nout; o0 += P2PM_BLOCK / S) {
+                const int o = o0 + tid / S, st = tid % S;
+                double v = 0.0;
+                if (o < nout) {
+                    const int t = o >> 2, comp = o & 3;
+                    const int gi = t % G, half = t / G;  // target t = gi + half * G
+                    const int row = 8 * half + 2 * comp;
+                    for (int r = st; r < R; r += S) {
+                        const int q = r * G + gi;
+                        v += (double)red[row][q] + (double)red[row + 1][q];
+                    }
                 }
-                if (nu == 1) {
-                    const uint32_t slot = tf + t0 + tid;
-                    ax[slot] = sacc[0];
-                    ay[slot] = sacc[1];
-                    az[slot] = sacc[2];
-                    pot[slot] = sacc[3];
-                } else {
-                    U.part[U.soff[c] + k * tn + t0 + tid] = make_double4(sacc[0], sacc[1], sacc[2], sacc[3]);
+                for (int w = S >> 1; w > 0; w >>= 1) v += __shfl_down_sync(0xffffffffu, v, w, S);
+                if (o < nout && st == 0) {
+                    const int t = o >> 2, comp = o & 3;
+                    if (nu == 1) {
+                        double* out = comp == 0 ? ax : comp == 1 ? ay : comp == 2 ? az : pot;
+                        out[tf + t0 + t] = v;
+                    } else {
+                        reinterpret_cast<double*>(U.part + U.soff[c] + k * tn + t0 + t)[comp] = v;
+                    }
                 }
             }
             __syncthreads();
