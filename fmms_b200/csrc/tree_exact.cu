@@ -956,6 +956,11 @@ __device__ __forceinline__ int warp_append(int* counter, bool mine, int lane) {
     return mine ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
 }
 
+// Latency: a walk iteration is a chain of dependent L2 round trips (the
+// frontier entry, then the cells, then the appends), so every read a pair can
+// need -- both cells' leaf flags, geometry and children -- is issued at once
+// after the entry, and the three appends (M2L, P2P, next frontier) are one
+// atomic instruction from three lanes.
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict__ pows,
                             const double* __restrict__ fminv, WalkBufs w, int cur) {
     // After an overflow the frontier holds unwritten entries: stop, the host
@@ -971,24 +976,28 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
     // whole warps step through the frontier together (the ballots need every lane)
     for (int q0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < nin; q0 += stride) {
         const int q = q0 + lane;
-        int kind = WK_NONE, a = 0, b = 0, sc = 0, npush = 0;
+        int kind = WK_NONE, a = 0, b = 0, npush = 0;
         bool split_a = false;
+        int cha[8], chb[8];
         if (q < nin) {
             const uint2 pr = fin[q];
             a = (int)pr.x;
             b = (int)pr.y;
             const bool la = cv.leaf[a], lb = cv.leaf[b];
+            const double4 ga = cv.geo[a], gb = cv.geo[b];
+            load_children(cv, a, cha);
+            load_children(cv, b, chb);
             if (a == b) {
                 if (la) {
                     kind = WK_P2P;
                 } else {
                     kind = WK_SPLIT_SELF;
-                    sc = a;
-                    const int nc = n_children(cv, a);
-                    npush = nc * (nc + 1) / 2;
+                    int nch = 0;
+#pragma unroll
+                    for (int o = 0; o < 8; ++o) nch += cha[o] >= 0;
+                    npush = nch * (nch + 1) / 2;
                 }
             } else {
-                const double4 ga = cv.geo[a], gb = cv.geo[b];
                 bool acc;
                 if (mp.mode == FMMX_MAC_DEHNEN)
                     acc = accept_dehnen(cv, mp, pows, fminv, a, b, ga, gb) &&
@@ -1003,21 +1012,15 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
                     // split b when a is a leaf or b is the larger cell, else split a
                     kind = WK_SPLIT;
                     split_a = lb || (!la && ga.w >= gb.w);
-                    sc = split_a ? a : b;
-                    npush = n_children(cv, sc);
+                    int nch = 0;
+#pragma unroll
+                    for (int o = 0; o < 8; ++o) nch += (split_a ? cha[o] : chb[o]) >= 0;
+                    npush = nch;
                 }
             }
         }
-        const int sm = warp_append(&w.counts[WC_M2L], kind == WK_M2L, lane);
-        if (kind == WK_M2L) {
-            if ((uint32_t)sm < w.cap_m2l) w.m2l[sm] = make_uint2(a, b);
-            else atomicOr(&w.counts[WC_OVERFLOW], 4);
-        }
-        const int sp = warp_append(&w.counts[WC_P2P], kind == WK_P2P, lane);
-        if (kind == WK_P2P) {
-            if ((uint32_t)sp < w.cap_p2p) w.p2p[sp] = make_uint2(a, b);
-            else atomicOr(&w.counts[WC_OVERFLOW], 2);
-        }
+        const unsigned mm = __ballot_sync(0xffffffffu, kind == WK_M2L);
+        const unsigned mq = __ballot_sync(0xffffffffu, kind == WK_P2P);
         // next frontier: inclusive prefix sum of the pushes across the warp
         int incl = npush;
         for (int o = 1; o < 32; o <<= 1) {
@@ -1025,30 +1028,46 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
             if (lane >= o) incl += t;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
+        // lanes 0, 1, 2 reserve the warp's M2L, P2P and frontier entries
+        int got = 0;
+        {
+            const int v = lane == 0 ? __popc(mm) : lane == 1 ? __popc(mq) : lane == 2 ? total : 0;
+            int* ctr = w.counts + (lane == 0 ? WC_M2L : lane == 1 ? WC_P2P : nxt);
+            if (v > 0) got = atomicAdd(ctr, v);
+        }
+        const int bm = __shfl_sync(0xffffffffu, got, 0);
+        const int bp = __shfl_sync(0xffffffffu, got, 1);
+        const int bf = __shfl_sync(0xffffffffu, got, 2);
+        const unsigned below = (1u << lane) - 1u;
+        if (kind == WK_M2L) {
+            const int sm = bm + __popc(mm & below);
+            if ((uint32_t)sm < w.cap_m2l) w.m2l[sm] = make_uint2(a, b);
+            else atomicOr(&w.counts[WC_OVERFLOW], 4);
+        } else if (kind == WK_P2P) {
+            const int sp = bp + __popc(mq & below);
+            if ((uint32_t)sp < w.cap_p2p) w.p2p[sp] = make_uint2(a, b);
+            else atomicOr(&w.counts[WC_OVERFLOW], 2);
+        }
         if (total == 0) continue;
-        int base = 0;
-        if (lane == 31) base = atomicAdd(&w.counts[nxt], total);
-        base = __shfl_sync(0xffffffffu, base, 31);
-        if ((uint32_t)(base + total) > w.cap_front) {
+        if ((uint32_t)(bf + total) > w.cap_front) {
             if (lane == 0) atomicOr(&w.counts[WC_OVERFLOW], 1);
             continue;
         }
-        int pos = base + incl - npush;
-        int ch[8];
-        if (npush) load_children(cv, sc, ch);
+        int pos = bf + incl - npush;
         if (kind == WK_SPLIT_SELF) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                if (ch[i] < 0) continue;
+                if (cha[i] < 0) continue;
 #pragma unroll
                 for (int j = i; j < 8; ++j)
-                    if (ch[j] >= 0) fout[pos++] = make_uint2(ch[i], ch[j]);
+                    if (cha[j] >= 0) fout[pos++] = make_uint2(cha[i], cha[j]);
             }
         } else if (kind == WK_SPLIT) {
 #pragma unroll
             for (int o = 0; o < 8; ++o) {
-                if (ch[o] < 0) continue;
-                fout[pos++] = split_a ? make_uint2(ch[o], b) : make_uint2(a, ch[o]);
+                const int c = split_a ? cha[o] : chb[o];
+                if (c < 0) continue;
+                fout[pos++] = split_a ? make_uint2(c, b) : make_uint2(a, c);
             }
         }
     }

@@ -79,6 +79,7 @@ ENGINE_BYTES_PER_BODY = 640
 SESSION_FIXED_BYTES = 1 << 20
 STAGED_BYTES_PER_BODY = 56  # pos, vel, mass staged on the device while queued
 SMALL_POOL_RESERVE = 256 << 20  # small-block pool reserved per stream (blocks <= 1 MB)
+ARENA_PLAN_SHARE = 0.8  # share of the staging arena that background staging may plan
 
 # Size classes (lower bounds of N) of the lanes: one lane by default.
 LANE_BOUNDS = (0,)
@@ -110,6 +111,7 @@ class Session:
     pending: tuple | None = dataclasses.field(default=None, repr=False)  # result copy job, host pos, host vel
     stage_job: object | None = dataclasses.field(default=None, repr=False)  # staging in progress
     planned: bool = False  # counted in the staging budget (queued for staging, staging, or staged)
+    stage_region: tuple | None = dataclasses.field(default=None, repr=False)  # (offset, bytes) in the arena
 
     @property
     def n(self) -> int:
@@ -122,7 +124,8 @@ class Session:
         """The same request, not yet served."""
         return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
                                    primed=False, last_end=0.0, retry_after=-1, step_ms=[], result_pos=None,
-                                   result_vel=None, staged=None, pending=None, stage_job=None, planned=False)
+                                   result_vel=None, staged=None, pending=None, stage_job=None, planned=False,
+                                   stage_region=None)
 
 
 def _interp_loglog(ns, vals, n):
@@ -133,6 +136,61 @@ def _interp_loglog(ns, vals, n):
         slope = max((lv[-1] - lv[-2]) / (ln[-1] - ln[-2]), 0.0)
         return float(np.exp(lv[-1] + slope * (x - ln[-1])))
     return float(np.exp(np.interp(x, ln, lv)))
+
+
+class DeviceArena:
+    """First-fit allocator over one device buffer allocated at start-up. The
+    bodies of queued sessions are staged here, so staging never calls the
+    caching allocator, which on a busy device fell back to cudaMalloc (or
+    freed cached segments, synchronising the device) and held the lane's
+    thread for 100-150 ms. A region given back is reused once the event
+    recorded with it (after the last read of the region) has completed."""
+
+    ALIGN = 256
+
+    def __init__(self, torch, dev, nbytes):
+        self.size = int(nbytes)
+        self.buf = torch.empty(self.size, dtype=torch.uint8, device=dev) if self.size > 0 else None
+        self.free = [(0, self.size)] if self.size > 0 else []  # (offset, bytes), by offset
+        self.pending = []  # (event, offset, bytes)
+        self.lock = threading.Lock()
+
+    def _put(self, off, size):
+        fr = self.free
+        i = 0
+        while i < len(fr) and fr[i][0] < off:
+            i += 1
+        fr.insert(i, (off, size))
+        if i + 1 < len(fr) and fr[i][0] + fr[i][1] == fr[i + 1][0]:  # merge with the next
+            fr[i] = (off, fr[i][1] + fr[i + 1][1])
+            del fr[i + 1]
+        if i > 0 and fr[i - 1][0] + fr[i - 1][1] == fr[i][0]:  # and with the previous
+            fr[i - 1] = (fr[i - 1][0], fr[i - 1][1] + fr[i][1])
+            del fr[i]
+
+    def alloc(self, nbytes):
+        """(offset, bytes) of a free region of at least nbytes, or None."""
+        nb = -(-int(nbytes) // self.ALIGN) * self.ALIGN
+        with self.lock:
+            keep = []
+            for ev, off, size in self.pending:
+                if ev is None or ev.query():
+                    self._put(off, size)
+                else:
+                    keep.append((ev, off, size))
+            self.pending = keep
+            for i, (off, size) in enumerate(self.free):
+                if size >= nb:
+                    if size == nb:
+                        del self.free[i]
+                    else:
+                        self.free[i] = (off + nb, size - nb)
+                    return off, nb
+        return None
+
+    def release(self, region, event=None):
+        with self.lock:
+            self.pending.append((event, region[0], region[1]))
 
 
 class CopyJob:
@@ -365,9 +423,15 @@ class Lane:
         pos = torch.cat([s.staged[0] for s in new])
         vel = torch.cat([s.staged[1] for s in new])
         mass = torch.cat([s.staged[2] for s in new])
+        done = torch.cuda.Event()
+        done.record(self.stream)  # after the copies out of the staged buffers
         for s in new:
-            for t in s.staged[:3]:
-                t.record_stream(self.stream)
+            if s.stage_region is not None:
+                self.srv.arena.release(s.stage_region, done)
+                s.stage_region = None
+            else:
+                for t in s.staged[:3]:
+                    t.record_stream(self.stream)
             s.staged = None
         self.srv.unstage(sum(s.n for s in new))
         acc = torch.zeros_like(pos)
@@ -502,6 +566,10 @@ class Lane:
                     self.recent_ratio.append(max(s.step_ms[-1] / self.srv.model.iso(s.n) for s in stepping))
             joined = [s for s in self.members if not s.primed]
             model = self.srv.model
+            if predicted and stepping and not joined and model is not None:
+                # the first step of a batch started in an empty lane: learn
+                # from its prediction as from a join
+                self.corr = min(4.0, max(1.0, 0.9 * self.corr, self.last_interval_ms / predicted))
             if joined and model is not None and stepping:
                 # a join into a running batch: this tick is a step interval of
                 # the sessions already stepping. Learn how far the model
@@ -538,8 +606,9 @@ class Server:
     headroom: the bound used for admission decisions (below latency_slo, to
     leave room for prediction error).
     stage_limit_bytes: device bytes of queued sessions' bodies staged ahead of
-    their admission (sessions beyond it are staged when they join); also the
-    allocator pool reserved on the copy stream.
+    their admission (sessions beyond it are staged when they join); the
+    staging arena, allocated at start-up, holds stage_limit_bytes /
+    ARENA_PLAN_SHARE.
     lane_reserve_bytes: allocator pool reserved on each lane's stream.
     refresh_every: a lane's forest is rebuilt whenever its members change and
     otherwise every refresh_every ticks; in between the tree and interaction
@@ -589,13 +658,17 @@ class Server:
             prio = max(greatest, least - (len(bounds) - 1 - i)) if greatest < least else least
             # with several lanes, short M2L blocks let the higher-priority lanes in
             self.lanes.append(Lane(self, lo, prio, preemptible=len(bounds) > 1))
-        # Device allocations in the steady state come from the caching
-        # allocator's pools, one per stream and size class (blocks up to 1 MB
-        # are carved from 2 MB segments, larger ones from their own): reserve
-        # both up front (allocate and free once), so that staging, joins and
-        # kicks do not reach cudaMalloc, which was seen to take ~90 ms at times
-        # on a busy device, even for a 2 MB segment.
-        for st, nbytes in [(self.copy_stream, self.stage_limit)] + [(ln.stream, lane_reserve_bytes) for ln in self.lanes]:
+        # Staged bodies live in the arena. The lanes' own allocations (joins,
+        # kicks, departures) come from the caching allocator's pools, one per
+        # stream and size class (blocks up to 1 MB are carved from 2 MB
+        # segments, larger ones from their own): reserve both up front
+        # (allocate and free once), so that they do not reach cudaMalloc,
+        # which was seen to take ~90 ms at times on a busy device, even for a
+        # 2 MB segment.
+        # staging ahead fills the arena up to ARENA_PLAN_SHARE of it: the rest
+        # is for sessions that join before their background copy began
+        self.arena = DeviceArena(torch, self.dev, self.stage_limit / ARENA_PLAN_SHARE)
+        for st, nbytes in [(ln.stream, lane_reserve_bytes) for ln in self.lanes]:
             if nbytes > 0:
                 with torch.cuda.stream(st):
                     blk = torch.empty(int(nbytes), dtype=torch.uint8, device=self.dev)
@@ -671,14 +744,29 @@ class Server:
     def mem_used(self) -> float:
         return self.used
 
-    def _start_staging(self, s: Session):
+    def _start_staging(self, s: Session, wait: bool = False) -> bool:
+        """Place the session's device buffers (in the arena; with wait, from
+        the caching allocator when the arena has no room) and prepare the
+        copy; False if there is no room now."""
         torch = self.torch
         t0 = time.perf_counter()
-        with torch.cuda.stream(self.copy_stream):
-            dev = [torch.empty(tuple(np.shape(a)), dtype=torch.float64, device=self.dev) for a in (s.pos, s.vel, s.mass)]
-        self.copy_log.append((t0, time.perf_counter(), "alloc", s.n * STAGED_BYTES_PER_BODY))
+        n = s.n
+        region = self.arena.alloc(STAGED_BYTES_PER_BODY * n)
+        if region is not None:
+            seg = self.arena.buf[region[0]:region[0] + STAGED_BYTES_PER_BODY * n]
+            dev = [seg[:24 * n].view(torch.float64).view(n, 3), seg[24 * n:48 * n].view(torch.float64).view(n, 3),
+                   seg[48 * n:56 * n].view(torch.float64)]
+            s.stage_region = region
+        elif wait:
+            with torch.cuda.stream(self.copy_stream):
+                dev = [torch.empty(tuple(np.shape(a)), dtype=torch.float64, device=self.dev)
+                       for a in (s.pos, s.vel, s.mass)]
+        else:
+            return False
+        self.copy_log.append((t0, time.perf_counter(), "alloc", n * STAGED_BYTES_PER_BODY))
         host = [_u8(np.ascontiguousarray(a, dtype=np.float64)) for a in (s.pos, s.vel, s.mass)]
         s.stage_job = (CopyJob([(h, _u8(d)) for h, d in zip(host, dev)], to_device=True), dev, time.perf_counter())
+        return True
 
     def _end_staging(self, s: Session):
         torch = self.torch
@@ -705,7 +793,7 @@ class Server:
                 self.staged_bytes += s.n * STAGED_BYTES_PER_BODY
                 s.planned = True
         if s.stage_job is None:
-            self._start_staging(s)
+            self._start_staging(s, wait=True)
         self.ring.finish(s.stage_job[0], self.copy_stream)
         self._end_staging(s)
 
@@ -752,8 +840,12 @@ class Server:
         if s is None:
             return False
         if s.staged is None:
-            if s.stage_job is None:
-                self._start_staging(s)
+            if s.stage_job is None and not self._start_staging(s):
+                with self.lock:  # no room in the arena yet: retry once a region comes back
+                    if self.staging is s:
+                        self.staging = None
+                        self.to_stage.appendleft(s)
+                return False
             if not self.ring.advance(s.stage_job[0], self.copy_stream):
                 return True
             self._end_staging(s)

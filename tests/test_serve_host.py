@@ -11,7 +11,7 @@ from types import SimpleNamespace
 import numpy as np
 import pytest
 
-from fmms_b200.serve import TICK_FIELDS, Lane, LatencyModel, Session, worst_intervals
+from fmms_b200.serve import TICK_FIELDS, DeviceArena, Lane, LatencyModel, Session, worst_intervals
 
 
 def session(sid, n, submitted_at=0.0, staged=True):
@@ -178,3 +178,30 @@ def test_worst_intervals_split_and_copy_overlap():
     assert top["copy_overlap_ms"] == pytest.approx(37.2)
     assert top["copies"] == [["stage", pytest.approx(0.7), pytest.approx(37.2), 5.0]]
     assert w[1]["interval_ms"] == pytest.approx(3.0) and w[1]["copy_overlap_ms"] == 0.0
+
+
+def test_arena_first_fit_reuse_and_coalescing():
+    """The staging arena hands out 256-byte aligned regions first fit, reuses
+    a region only once its event has completed, and merges neighbours."""
+    import torch
+
+    class Ev:
+        def __init__(self, done):
+            self.done = done
+
+        def query(self):
+            return self.done
+
+    a = DeviceArena(torch, "cpu", 4096)
+    r1, r2, r3 = a.alloc(1000), a.alloc(1024), a.alloc(2000)
+    assert r1 == (0, 1024) and r2 == (1024, 1024) and r3 == (2048, 2048)
+    assert a.alloc(1) is None  # full
+    pending = Ev(False)
+    a.release(r2, pending)
+    assert a.alloc(256) is None  # the reader of r2 has not finished
+    pending.done = True
+    assert a.alloc(256) == (1024, 256)
+    a.release((1024, 256))
+    a.release(r1)
+    a.release(r3)
+    assert a.alloc(4096) == (0, 4096)  # all merged back into one region
