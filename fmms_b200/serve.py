@@ -40,8 +40,10 @@ sessions finish) scales later predictions, and if it took longer than
 `headroom` times the isolated latency of the batch's smallest session, the
 sessions that joined in it -- which have not stepped yet, so nothing of theirs
 changes -- go back to the front of the queue and wait for a session of the
-lane to finish before they are tried again. Sessions that start together in an
-empty lane are bounded by the model alone (their joining tick, with the
+lane to finish before they are tried again. A running batch in which a session
+has already had a step over `latency_slo` times its isolated latency takes no
+more joins (its p99 allows one such step in a hundred). Sessions that start
+together in an empty lane are bounded by the model alone (their joining tick, with the
 one-time costs of joining, is no session's step). Only the first session of an
 empty lane may join before the background copies have put its bodies on the
 device. The queue is scanned in arrival
@@ -111,6 +113,7 @@ class Session:
     pending: tuple | None = dataclasses.field(default=None, repr=False)  # result copy job, host pos, host vel
     stage_job: object | None = dataclasses.field(default=None, repr=False)  # staging in progress
     planned: bool = False  # counted in the staging budget (queued for staging, staging, or staged)
+    slow_steps: int = 0  # steps that took longer than latency_slo times its isolated latency
     stage_region: tuple | None = dataclasses.field(default=None, repr=False)  # (offset, bytes) in the arena
 
     @property
@@ -125,7 +128,7 @@ class Session:
         return dataclasses.replace(self, submitted_at=None, admitted_at=None, finished_at=None, steps_done=0,
                                    primed=False, last_end=0.0, retry_after=-1, step_ms=[], result_pos=None,
                                    result_vel=None, staged=None, pending=None, stage_job=None, planned=False,
-                                   stage_region=None)
+                                   stage_region=None, slow_steps=0)
 
 
 def _interp_loglog(ns, vals, n):
@@ -376,6 +379,11 @@ class Lane:
         new = []
         if not srv.gate_open(self):
             return new
+        if model is not None and any(m.slow_steps for m in self.members):
+            # a join stretches the tick it happens in; a session's p99 step
+            # latency allows one such step in a hundred, so a batch one of
+            # whose sessions already had a slow step takes no more joins
+            return new
         # predicted step latency of the batch as it stands, and its smallest member
         tau = self.predicted_ms if self.predicted_ms is not None else self.last_interval_ms
         nmin = min((s.n for s in self.members), default=None)
@@ -558,6 +566,9 @@ class Lane:
                 s.step_ms.append(1e3 * (t_end - s.last_end))
                 s.last_end = t_end
                 self.bodies_stepped += s.n
+                if self.srv.model is not None and self.srv.latency_slo is not None and \
+                        s.step_ms[-1] > self.srv.latency_slo * self.srv.model.iso(s.n):
+                    s.slow_steps += 1
             predicted = self.predicted_ms
             if stepping:
                 self.last_interval_ms = max(s.step_ms[-1] for s in stepping)

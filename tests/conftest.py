@@ -13,6 +13,21 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: larger CPU cases")
 
 
+def published():
+    """The reference's published results for its force path (golden values,
+    tests/golden/reference_published.json, written by make_published.py from
+    the reference's own text files)."""
+    import json
+
+    with open(os.path.join(ROOT, "tests", "golden", "reference_published.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return published()
+
+
 @pytest.fixture(scope="session")
 def orc():
     import oracle

@@ -284,3 +284,37 @@ def test_c3_clusters_plain(orc):
     rp = rel_rows(res.pot, pot_o)
     assert ra.max() < ACC_TOL, f"acc rel err {ra.max():.3e}"
     assert rp.max() < ACC_TOL, f"pot rel err {rp.max():.3e}"
+
+
+def test_walk_statistics_n1e6_published(orc, golden):
+    """The engine's dual walk at the reference's published walk statistics
+    (golden values: 205,395 leaves, 26.7M pops, 20.6M M2L pairs, 2.60M P2P
+    leaf-pair calls at N = 1e6, plummer(n, 0, 42), p = 8, eps = 1e-5, leaf
+    16; PERF-ANALYSIS.md:50-52)."""
+    import fmms_b200 as fx
+
+    g = golden["walk_stats_n1e6"]
+    mass, pos = orc.plummer(1_000_000, seed=42)
+    f = fx.Fmm(mass, pos, 8, 1e-5, 16)
+    f.run()
+    st = f.stats()
+    leaves = int(st["n_leaves"])
+    assert leaves == g["leaves"]
+    assert round(st["walk_pops"] / 1e6, 1) == g["pops_millions"]
+    assert round(st["n_m2l"] / 1e6, 1) == g["m2l_pairs_millions"]
+    assert round((st["n_p2p"] - leaves) / 1e6, 2) == g["p2p_calls_millions"]
+
+
+def test_exit_gate_n1e4_published(orc, golden):
+    """tests/exit_gate.rs:11-24 on the device: the scaled errors against the
+    direct sum reproduce the reference's published release run (todo.md:586)
+    to its printed digits."""
+    import fmms_b200 as fx
+
+    g = golden["exit_gate_n1e4"]
+    mass, pos = orc.plummer(10_000, seed=2024)
+    acc = fx.Fmm(mass, pos, 5, 1e-5, 32).run().accel
+    a_ref, _ = orc.direct(mass, pos)
+    max_s, _, rms_s, _ = orc.scaled_error(a_ref, acc, mass, pos)
+    assert round(max_s, g["printed_digits"]["max_s"]) == g["max_s"], max_s
+    assert round(rms_s, g["printed_digits"]["rms_s"]) == g["rms_s"], rms_s

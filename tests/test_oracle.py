@@ -379,7 +379,7 @@ def test_hernquist_smoke(orc):
 
 
 @pytest.mark.slow
-def test_exit_gate_n1e4(orc):
+def test_exit_gate_n1e4(orc, golden):
     """tests/exit_gate.rs:11-24 (ignored in the reference; reported there as
     rms 4.87e-5, max 1.83e-3)."""
     mass, pos = orc.plummer(10_000, seed=2024)
@@ -388,14 +388,15 @@ def test_exit_gate_n1e4(orc):
     a_ref, _ = orc.direct(mass, pos)
     max_s, _, rms_s, _ = orc.scaled_error(a_ref, acc, mass, pos)
     assert rms_s < 1e-4 and max_s < 1e-2
-    # the reference's published release run of this gate, todo.md:586:
-    # "max_s 1.826e-3, rms_s 4.867e-5", to the printed digits
-    assert round(max_s, 6) == 1.826e-3, max_s
-    assert round(rms_s, 8) == 4.867e-5, rms_s
+    # the reference's published release run of this gate (todo.md:586), to
+    # the printed digits (tests/golden/reference_published.json)
+    g = golden["exit_gate_n1e4"]
+    assert round(max_s, g["printed_digits"]["max_s"]) == g["max_s"], max_s
+    assert round(rms_s, g["printed_digits"]["rms_s"]) == g["rms_s"], rms_s
 
 
 @pytest.mark.slow
-def test_walk_statistics_n1e6(orc):
+def test_walk_statistics_n1e6(orc, golden):
     """The reference's published walk statistics of one force evaluation at
     N = 1e6 (PERF-ANALYSIS.md:50-52, measured by the bench profile mode,
     crates/bench/src/main.rs:554-641, on plummer(n, 0, 42), p = 8,
@@ -407,10 +408,11 @@ def test_walk_statistics_n1e6(orc):
     f = orc.Fmm(mass, pos, 8, 1e-5, 16)
     n_m2l, n_p2p, pops = f.walk(nthreads=os.cpu_count() or 1)
     leaves = int(f.cells()["leaf"].sum())
-    assert leaves == 205_395
-    assert round(pops / 1e6, 1) == 26.7
-    assert round(n_m2l / 1e6, 1) == 20.6
-    assert round((n_p2p - leaves) / 1e6, 2) == 2.60
+    g = golden["walk_stats_n1e6"]
+    assert leaves == g["leaves"]
+    assert round(pops / 1e6, 1) == g["pops_millions"]
+    assert round(n_m2l / 1e6, 1) == g["m2l_pairs_millions"]
+    assert round((n_p2p - leaves) / 1e6, 2) == g["p2p_calls_millions"]
 
 
 def test_extensions_softening_and_theta(orc):

@@ -205,3 +205,16 @@ def test_arena_first_fit_reuse_and_coalescing():
     a.release(r1)
     a.release(r3)
     assert a.alloc(4096) == (0, 4096)  # all merged back into one region
+
+
+def test_admission_no_joins_after_a_slow_step():
+    """A session's p99 step latency allows one slow step in a hundred: a
+    running batch one of whose sessions already had a step over the latency
+    target takes no more joins (they would stretch another of its steps)."""
+    member = session(9, 1000)
+    member.slow_steps = 1
+    ln = fake_lane([session(0, 1000)], members=[member])
+    ln.last_interval_ms = 1.01
+    assert Lane.admit(ln, now=0.0) == []
+    member.slow_steps = 0
+    assert len(Lane.admit(ln, now=0.0)) == 1
