@@ -218,6 +218,8 @@ struct fmmx_ctx {
     DBuf<uint32_t> m2l_off, p2p_off, list_cnt;               // nc + 1 each
     DBuf<int> m2l_longs, p2p_longs;                         // long-segment lists, 2 nc + 128 each
     DBuf<uint32_t> long_bounds;
+    DBuf<char> cub_tmp2;                // the M2L list's sort scratch (built beside the P2P)
+    DBuf<uint32_t> list_cnt2, long_bounds2;
     // near-field work units of the mixed P2P (per leaf: units, scratch bodies)
     DBuf<uint32_t> p2p_units, p2p_scr, p2p_uoff, p2p_soff;
     DBuf<double4> p2p_part;
@@ -695,40 +697,42 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
     }
 }
 
-fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
+// The directed lists of one kind (M2L or P2P) from the walk's mutual pairs:
+// a counting sort on the destination, segment sorts, and -- after a host
+// read-back of the number of long segments -- CUB's segmented sort of those.
+// The two kinds run on different streams with their own scratch (tmp, cnt,
+// bounds), so that the P2P can start while the M2L list is being built.
+fmmx_status build_list(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp, DBuf<uint32_t>& cnt,
+                       DBuf<uint32_t>& bounds) {
     const int nc = ctx->nc;
-    const int nm = ctx->n_m2l, np = ctx->n_p2p;
-    const size_t n_m2l_dir = 2 * (size_t)nm;
-    const size_t n_p2p_dir = np > 0 ? 2 * (size_t)np - (size_t)ctx->nleaves : 0;  // one entry per leaf self pair
-    if (n_m2l_dir > 0x7fffffffull || n_p2p_dir > 0x7fffffffull)
-        return fail(ctx, FMMX_OUT_OF_MEMORY, "interaction lists above 2^31 entries");
-    CK(ctx->m2l_off.ensure(nc + 1), "alloc lists");
-    CK(ctx->p2p_off.ensure(nc + 1), "alloc lists");
-    CK(ctx->list_cnt.ensure(nc + 1), "alloc lists");
-    CK(ctx->m2l_src_u.ensure(std::max<size_t>(n_m2l_dir, 1)), "alloc lists");
-    CK(ctx->m2l_src.ensure(std::max<size_t>(n_m2l_dir, 1)), "alloc lists");
-    // (room for 2 entries per pair: the scatter writes inside the counted
-    // segments whatever the number of self pairs)
-    CK(ctx->p2p_src_u.ensure(std::max<size_t>(2 * (size_t)np, 1)), "alloc lists");
-    CK(ctx->p2p_src.ensure(std::max<size_t>(2 * (size_t)np, 1)), "alloc lists");
-    CK(ctx->inter.ensure(1), "alloc");
-    CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
-    const size_t tb = std::max(directed_list_temp((int)n_m2l_dir, nc), directed_list_temp((int)n_p2p_dir, nc));
-    CK(ctx->cub_tmp.ensure(tb), "alloc sort");
-    CK(ctx->m2l_longs.ensure(2 * (size_t)nc + 128), "alloc lists");
-    CK(ctx->p2p_longs.ensure(2 * (size_t)nc + 128), "alloc lists");
-    LCOUNT(12);  // per list: count, scan (2), scatter, segment sorts (2)
-    CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l.p, nm, (int)n_m2l_dir, nc, nullptr, nullptr,
-                           ctx->list_cnt.p, ctx->m2l_off.p, ctx->m2l_src_u.p, ctx->m2l_src.p, ctx->m2l_longs.p,
-                           grid_for(nm, 256), s),
-       "m2l lists");
-    CK(build_directed_list(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p.p, np, (int)n_p2p_dir, nc, ctx->c_count.p,
-                           ctx->inter.p, ctx->list_cnt.p, ctx->p2p_off.p, ctx->p2p_src_u.p, ctx->p2p_src.p,
-                           ctx->p2p_longs.p, grid_for(np, 256), s),
-       "p2p lists");
-    CKL("lists");
-    const bool mixed = ctx->cfg.precision == FMMX_MIXED;
-    if (mixed) {
+    const int npairs = near ? ctx->n_p2p : ctx->n_m2l;
+    const size_t ndir = near ? (npairs > 0 ? 2 * (size_t)npairs - (size_t)ctx->nleaves : 0)  // one entry per self pair
+                             : 2 * (size_t)npairs;
+    if (ndir > 0x7fffffffull) return fail(ctx, FMMX_OUT_OF_MEMORY, "interaction lists above 2^31 entries");
+    DBuf<uint32_t>& off = near ? ctx->p2p_off : ctx->m2l_off;
+    DBuf<uint32_t>& src_u = near ? ctx->p2p_src_u : ctx->m2l_src_u;
+    DBuf<uint32_t>& src = near ? ctx->p2p_src : ctx->m2l_src;
+    DBuf<int>& longs = near ? ctx->p2p_longs : ctx->m2l_longs;
+    CK(off.ensure(nc + 1), "alloc lists");
+    CK(cnt.ensure(nc + 1), "alloc lists");
+    // (P2P: room for 2 entries per pair -- the scatter writes inside the
+    // counted segments whatever the number of self pairs)
+    const size_t room = near ? 2 * (size_t)npairs : ndir;
+    CK(src_u.ensure(std::max<size_t>(room, 1)), "alloc lists");
+    CK(src.ensure(std::max<size_t>(room, 1)), "alloc lists");
+    CK(longs.ensure(2 * (size_t)nc + 128), "alloc lists");
+    if (near) {
+        CK(ctx->inter.ensure(1), "alloc");
+        CK(cudaMemsetAsync(ctx->inter.p, 0, sizeof(unsigned long long), s), "memset");
+    }
+    CK(tmp.ensure(directed_list_temp((int)ndir, nc)), "alloc sort");
+    LCOUNT(6);  // count, scan (2), scatter, segment sorts (2)
+    CK(build_directed_list(tmp.p, tmp.cap, near ? ctx->p2p.p : ctx->m2l.p, npairs, (int)ndir, nc,
+                           near ? ctx->c_count.p : nullptr, near ? ctx->inter.p : nullptr, cnt.p, off.p, src_u.p,
+                           src.p, longs.p, grid_for(npairs, 256), s),
+       near ? "p2p lists" : "m2l lists");
+    const bool units = near && ctx->cfg.precision == FMMX_MIXED;
+    if (units) {
         // near-field work units: per leaf ceil(sources / P2P_UNIT_SRC), and the
         // scratch for the partial sums of leaves with several units
         for (DBuf<uint32_t>* b : {&ctx->p2p_units, &ctx->p2p_scr, &ctx->p2p_uoff, &ctx->p2p_soff})
@@ -736,45 +740,36 @@ fmmx_status lists_impl(fmmx_ctx* ctx, cudaStream_t s) {
         CK(ctx->p2p_next.ensure(1), "alloc lists");
         const DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
         launch_p2p_plan(grid_for(nc + 1, 256), s, nc, lp, ctx->c_count.p, ctx->p2p_units.p, ctx->p2p_scr.p);
-        CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_units.p, ctx->p2p_uoff.p, nc + 1, s), "p2p units");
-        CK(scan_u32(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
+        CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_units.p, ctx->p2p_uoff.p, nc + 1, s), "p2p units");
+        CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
         LCOUNT(5);
     }
-    // host read-back: the number of long segments of each list and the P2P scratch size
-    int nlong_m = 0, nlong_p = 0;
+    // host read-back: the number of long segments (and the P2P scratch size)
+    int nlong = 0;
     uint32_t nscr = 0;
-    CK(cudaMemcpyAsync(&nlong_m, ctx->m2l_longs.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
-    CK(cudaMemcpyAsync(&nlong_p, ctx->p2p_longs.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
-    if (mixed) CK(cudaMemcpyAsync(&nscr, ctx->p2p_soff.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
+    CK(cudaMemcpyAsync(&nlong, longs.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+    if (units) CK(cudaMemcpyAsync(&nscr, ctx->p2p_soff.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
     CK(cudaStreamSynchronize(s), "lists");
-    if (mixed) CK(ctx->p2p_part.ensure(std::max<size_t>(nscr, 1)), "alloc p2p scratch");
-    if (nlong_m + nlong_p > 0) {
+    if (units) CK(ctx->p2p_part.ensure(std::max<size_t>(nscr, 1)), "alloc p2p scratch");
+    if (nlong > 0) {
         const int end_bit = bits_for((uint64_t)nc);
-        CK(ctx->long_bounds.ensure(2 * (size_t)std::max(nlong_m, nlong_p)), "alloc lists");
-        const size_t lt = std::max(long_segments_temp((int)n_m2l_dir, nlong_m, end_bit),
-                                   long_segments_temp((int)n_p2p_dir, nlong_p, end_bit));
-        CK(ctx->cub_tmp.ensure(lt), "alloc sort");
-        LCOUNT(2 * ((nlong_m > 0) + (nlong_p > 0)));
-        CK(sort_long_segments(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->m2l_off.p, ctx->m2l_longs.p, nlong_m,
-                              ctx->m2l_src_u.p, ctx->m2l_src.p, (int)n_m2l_dir, end_bit, ctx->long_bounds.p, s),
-           "m2l lists");
-        CK(sort_long_segments(ctx->cub_tmp.p, ctx->cub_tmp.cap, ctx->p2p_off.p, ctx->p2p_longs.p, nlong_p,
-                              ctx->p2p_src_u.p, ctx->p2p_src.p, (int)n_p2p_dir, end_bit, ctx->long_bounds.p, s),
-           "p2p lists");
+        CK(bounds.ensure(2 * (size_t)nlong), "alloc lists");
+        CK(tmp.ensure(long_segments_temp((int)ndir, nlong, end_bit)), "alloc sort");
+        LCOUNT(2);
+        CK(sort_long_segments(tmp.p, tmp.cap, off.p, longs.p, nlong, src_u.p, src.p, (int)ndir, end_bit, bounds.p,
+                              s),
+           near ? "p2p lists" : "m2l lists");
     }
     return FMMX_OK;
 }
 
-// Mixed form: FP32 M2L/L2L/L2P on normalised expansions, FP32 + double-single
-// P2P; events 5..9 as in the plain path.
-fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirList& lp, double* d_acc,
-                                    double* d_pot, bool tm) {
-    cudaStream_t s = ctx->stream, s2 = ctx->cfg.overlap ? ctx->stream2 : ctx->stream;
-    const int p = ctx->cfg.p, nc = ctx->nc;
+// Mixed form, near field: FP32 + double-single P2P on the second stream.
+fmmx_status near_mixed(fmmx_ctx* ctx, const DirList& lp, bool tm) {
+    cudaStream_t s2 = ctx->cfg.overlap ? ctx->stream2 : ctx->stream;
+    const int nc = ctx->nc;
     const size_t n = ctx->n;
     const CellsView cv = view(ctx);
     cudaEvent_t* ev = ctx->ev;
-    // near field on the second stream, beside the far field
     if (tm) CK(cudaEventRecord(ev[12], s2), "event");
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
     CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
@@ -785,6 +780,17 @@ fmmx_status evaluate_far_near_mixed(fmmx_ctx* ctx, const DirList& lm, const DirL
     CKL("p2p (mixed)");
     if (tm) CK(cudaEventRecord(ev[8], s2), "event");
     CK(cudaEventRecord(ctx->fork[2], s2), "event");
+    return FMMX_OK;
+}
+
+// Mixed form, far field: FP32 M2L/L2L on normalised expansions, then the L2P,
+// which adds the near field.
+fmmx_status far_mixed(fmmx_ctx* ctx, const DirList& lm, double* d_acc, double* d_pot, bool tm) {
+    cudaStream_t s = ctx->stream;
+    const int p = ctx->cfg.p, nc = ctx->nc;
+    const size_t n = ctx->n;
+    const CellsView cv = view(ctx);
+    cudaEvent_t* ev = ctx->ev;
     if (tm) CK(cudaEventRecord(ev[11], s), "event");  // far field from here
     CK(cudaMemsetAsync(ctx->loc_f.p, 0, (size_t)nc * half_stride(p) * sizeof(zf), s), "memset");
     if (ctx->n_m2l > 0) {
@@ -947,21 +953,22 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     }
     if (tm) CK(cudaEventRecord(ev[4], s2), "event");
     if (!reuse) {
-        fmmx_status st = lists_impl(ctx, s2);
+        CK(cudaEventRecord(ctx->fork[1], s2), "event");  // the walk's pairs are in place
+        fmmx_status st = build_list(ctx, true, s2, ctx->cub_tmp, ctx->list_cnt, ctx->long_bounds);
         if (st != FMMX_OK) return st;
-        ctx->lists_valid = true;
     }
     if (tm) CK(cudaEventRecord(ev[5], s2), "event");
-    CK(cudaEventRecord(ctx->fork[1], s2), "event");
-    CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L reads the lists
 
-    DirList lm{nullptr, ctx->m2l_src.p, ctx->m2l_off.p, ctx->m2l_off.p + 1, 32};
-    DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
+    // (each list's pointers are taken after its build, which may reallocate it)
+    const DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
+    // The near field starts on the second stream as soon as its list is
+    // built; the far field's list is built on the first stream after it is
+    // queued (beside the plain form's P2P; the mixed form's persistent P2P
+    // fills every SM, so there the list kernels follow it).
     if (mixed) {
-        fmmx_status ms = evaluate_far_near_mixed(ctx, lm, lp, d_acc, d_pot, tm);
+        fmmx_status ms = near_mixed(ctx, lp, tm);
         if (ms != FMMX_OK) return ms;
     } else {
-    {  // near field on the second stream, beside the far field
         if (tm) CK(cudaEventRecord(ev[12], s2), "event");
         const double soft2 = ctx->cfg.softening * ctx->cfg.softening;
         k_p2p_f64<<<(unsigned)nc, 128, 0, s2>>>(lp, nc, cv, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, soft2,
@@ -970,6 +977,19 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         if (tm) CK(cudaEventRecord(ev[8], s2), "event");
         CK(cudaEventRecord(ctx->fork[2], s2), "event");
     }
+    if (!reuse) {
+        CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L list reads the walk's pairs
+        if (tm) CK(cudaEventRecord(ev[14], s), "event");
+        fmmx_status st = build_list(ctx, false, s, ctx->cub_tmp2, ctx->list_cnt2, ctx->long_bounds2);
+        if (st != FMMX_OK) return st;
+        if (tm) CK(cudaEventRecord(ev[15], s), "event");
+        ctx->lists_valid = true;
+    }
+    const DirList lm{nullptr, ctx->m2l_src.p, ctx->m2l_off.p, ctx->m2l_off.p + 1, 32};
+    if (mixed) {
+        fmmx_status ms = far_mixed(ctx, lm, d_acc, d_pot, tm);
+        if (ms != FMMX_OK) return ms;
+    } else {
     if (tm) CK(cudaEventRecord(ev[11], s), "event");  // far field from here
     CK(cudaMemsetAsync(ctx->locals.p, 0, (size_t)nc * dim * sizeof(zd), s), "memset");
     if (ctx->n_m2l > 0) {
@@ -1026,7 +1046,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         // stages on the two streams overlap: each is timed on its own stream
         ctx->st.ms_upward = el(2, 3);
         ctx->st.ms_walk = el(10, 4);
-        ctx->st.ms_lists = el(4, 5);
+        ctx->st.ms_lists = el(4, 5) + (reuse ? 0.0 : el(14, 15));
         ctx->st.ms_m2l = el(11, 6);
         ctx->st.ms_l2l = el(6, 7);
         ctx->st.ms_p2p = el(12, 8);

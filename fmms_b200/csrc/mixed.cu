@@ -847,7 +847,11 @@ void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const
 template <int TILE>
 static void launch_tile(int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, const float4* loc,
                         float soft2, double* ax, double* ay, double* az, double* pot) {
-    int per_sm = 0;  // persistent blocks: as many as fit on an SM at once
+    // persistent blocks: as many as fit on an SM at once (capping them at four
+    // to leave room for the far field's list kernels beside the P2P was
+    // measured: the P2P lost more, 31.5 -> 35.8 ms at the clustered
+    // N = 2^22 workload, than the lists gained)
+    int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2p_mixed<TILE>, P2PM_BLOCK, 0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;

@@ -110,8 +110,10 @@ def test_mixed_p2p_giant_leaf_and_tiles(tile):
     """A leaf far above the leaf capacity (5000 bodies inside a cube of side
     1e-9, below the tree's finest level) next to an ordinary Plummer sphere:
     the near field takes such a leaf as a chunk of its own (more bodies than
-    its shared-memory leaf table holds), and tiles of 128 and 512 bodies give
-    forces within the FP32 floor of the FP64 direct sum."""
+    its shared-memory leaf table holds). With tiles of 128 and 512 bodies the
+    mixed form agrees with the plain FP64 form on the same tree and lists to
+    the FP32 floor (against the softened direct sum both forms carry the
+    unsoftened far field's error next to a unit mass in one point)."""
     import fmms_b200 as fx
 
     rng = np.random.default_rng(3)
@@ -119,14 +121,14 @@ def test_mixed_p2p_giant_leaf_and_tiles(tile):
     p2 = 0.5 + 1e-9 * rng.random((5000, 3))
     mass = np.concatenate([m1, np.full(5000, 1.0 / 5000)])
     pos = np.concatenate([p1, p2])
-    soft = 1e-2
-    g = fx.Fmm(mass, pos, 8, 0.0, 32, mac="theta", theta=0.5, softening=soft, precision="mixed", p2p_tile=tile)
+    kw = dict(mac="theta", theta=0.5, softening=1e-2)
+    g = fx.Fmm(mass, pos, 8, 0.0, 32, precision="mixed", p2p_tile=tile, **kw)
     res = g.run()
     assert g.stats()["n_leaves"] > 1
-    t = np.concatenate([targets(6000, 512), 6000 + targets(5000, 256)]).astype(np.uint32)
-    a_ref, pot_ref, _ = fx.direct_targets(mass, pos, t, softening=soft)
+    ref = fx.Fmm(mass, pos, 8, 0.0, 32, precision="plain", **kw).run()
     assert np.all(np.isfinite(res.accel)) and np.all(np.isfinite(res.pot))
-    e = rel_err(res.accel[t], a_ref)
-    assert np.percentile(e, 99) < 2e-5, np.percentile(e, 99)
-    pe = np.abs(res.pot[t] - pot_ref) / np.abs(pot_ref)
-    assert np.max(pe) < 1e-5, np.max(pe)
+    for part in (slice(0, 6000), slice(6000, 11000)):  # the sphere, the point mass
+        e = rel_err(res.accel[part], ref.accel[part])
+        assert np.percentile(e, 99) < 1e-5 and np.max(e) < 1e-4, (np.percentile(e, 99), np.max(e))
+        pe = np.abs(res.pot[part] - ref.pot[part]) / np.abs(ref.pot[part])
+        assert np.max(pe) < 1e-5, np.max(pe)
