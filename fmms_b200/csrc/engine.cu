@@ -1111,7 +1111,7 @@ fmmx_status fmmx_create(const fmmx_config* cfg, fmmx_ctx** out) {
     if (!(c.softening >= 0.0)) return FMMX_INVALID_ARG;
     if (c.center_mode != FMMX_CENTER_COM && c.center_mode != FMMX_CENTER_SPHERE) return FMMX_INVALID_ARG;
     if (c.precision != FMMX_PLAIN_FP64 && c.precision != FMMX_MIXED) return FMMX_INVALID_ARG;
-    if (c.p2p_tile < 0 || c.p2p_tile > 512) return FMMX_INVALID_ARG;
+    if (c.p2p_tile < 0 || c.p2p_tile > 1024) return FMMX_INVALID_ARG;
     if (c.preemptible != 0 && c.preemptible != 1) return FMMX_INVALID_ARG;
     if (!(c.soft_gap >= 0.0) || !std::isfinite(c.soft_gap)) return FMMX_INVALID_ARG;
     if (c.use_graphs != 0 && c.use_graphs != 1) return FMMX_INVALID_ARG;

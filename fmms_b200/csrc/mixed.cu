@@ -614,7 +614,11 @@ __global__ void __launch_bounds__(P2PM_BLOCK, 5) k_p2p_mixed(DirList L, int ncel
     constexpr int PPT = (NPAIR + P2PM_BLOCK - 1) / P2PM_BLOCK;  // pairs staged per thread
     __shared__ float4 ta[NPAIR];
     __shared__ float4 tz[NPAIR];
-    __shared__ float4 raw[P2PM_TILE];  // the next tile's bodies as copied (leaf-relative)
+    // the next tile's bodies as copied (leaf-relative); also the per-group
+    // sums at the end of a target chunk, when no copy is in flight
+    __shared__ float4 raw[P2PM_TILE > 512 ? P2PM_TILE : 512];
+    float(*red)[P2PM_BLOCK] = reinterpret_cast<float(*)[P2PM_BLOCK]>(raw);
+    static_assert(sizeof(raw) >= 16 * P2PM_BLOCK * sizeof(float), "the group sums alias the copy buffer");
     __shared__ uint32_t pre[P2PM_SRC_CHUNK + 1];
     __shared__ uint32_t sbase[P2PM_SRC_CHUNK];  // first slot of the leaf - its first position in the chunk
     __shared__ float4 soff[P2PM_SRC_CHUNK];     // source leaf centre - target leaf centre
@@ -622,7 +626,6 @@ __global__ void __launch_bounds__(P2PM_BLOCK, 5) k_p2p_mixed(DirList L, int ncel
     __shared__ uint32_t wsum[P2PM_BLOCK / 32];
     __shared__ int self_pos, nuse_sh;
     __shared__ uint32_t unit_sh;
-    __shared__ float red[16][P2PM_BLOCK];
     const int tid = threadIdx.x;
     const int lane = tid & 31, wid = tid >> 5;
     const uint32_t nunits = U.uoff[ncells];
@@ -864,7 +867,8 @@ void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, 
     k_local_coords<<<grid_for(n, 256), 256, 0, s>>>(n, body_leaf, cv, x, y, z, m, loc);
     if (tile <= 128) launch_tile<128>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
     else if (tile <= 256) launch_tile<256>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
-    else launch_tile<512>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
+    else if (tile <= 512) launch_tile<512>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
+    else launch_tile<1024>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
     k_p2p_combine<<<grid_for((size_t)ncells * 32, 256), 256, 0, s>>>(ncells, cv, U, ax, ay, az, pot);
 }
 

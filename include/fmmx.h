@@ -78,7 +78,7 @@ typedef struct fmmx_config {
     int m2l_kernel;    /* fmmx_m2l_kernel */
     int device;        /* CUDA device ordinal */
     void* stream;      /* cudaStream_t to run on, or NULL for a private stream */
-    int p2p_tile;      /* source bodies per shared-memory tile of the mixed P2P (128, 256, 512; 0 = 512) */
+    int p2p_tile;      /* source bodies per shared-memory tile of the mixed P2P (128, 256, 512, 1024; 0 = 512) */
     int preemptible;   /* 1: the M2L runs one short block per destination cell instead of persistent warps,
                           so kernels on higher-priority streams start between its blocks (serving lanes);
                           0 (default): persistent warps, the faster form for one evaluation at a time */

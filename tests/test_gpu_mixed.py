@@ -105,12 +105,12 @@ def test_mixed_full_size_c2():
         assert len(a) == len(b)
 
 
-@pytest.mark.parametrize("tile", [128, 512])
+@pytest.mark.parametrize("tile", [128, 512, 1024])
 def test_mixed_p2p_giant_leaf_and_tiles(tile):
     """A leaf far above the leaf capacity (5000 bodies inside a cube of side
     1e-9, below the tree's finest level) next to an ordinary Plummer sphere:
     the near field takes such a leaf as a chunk of its own (more bodies than
-    its shared-memory leaf table holds). With tiles of 128 and 512 bodies the
+    its shared-memory leaf table holds). With tiles of 128, 512 and 1024 bodies the
     mixed form agrees with the plain FP64 form on the same tree and lists to
     the FP32 floor (against the softened direct sum both forms carry the
     unsoftened far field's error next to a unit mass in one point)."""
