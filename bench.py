@@ -917,7 +917,12 @@ def run_ensemble(args, cfg, rank, world, local_rank):
             "vs_baseline": None, "data": "synthetic", "dtype": "f64" if args.precision == "plain" else "f32+f64",
             "config": {"workload": f"{args.nsys} Plummer systems, N log-uniform[1e3,1e5] (total {n}), one forest",
                        "p": p_use, "n_leaf": n_leaf, "p2p_tile": tile, "theta": theta, "soft_gap": gap,
-                       "autotune": {k: v for k, v in (tune or {}).items() if k != "candidates"}},
+                       "autotune": {k: v for k, v in (tune or {}).items() if k != "candidates"},
+                       "autotune_candidates": [[c["theta"], c["soft_gap"], c["p"], c["n_leaf"], c["p2p_tile"],
+                                                round(c["ms"], 2), float("%.3g" % c["err_p99_worst"])]
+                                               for c in (tune or {}).get("candidates", [])],
+                       "autotune_candidate_fields": ["theta", "soft_gap", "p", "n_leaf", "p2p_tile",
+                                                     "ms (sampled forest)", "p99 err (worst sampled system)"]},
             "per_system_force_err_p99": {"median": float(np.median(p99s)), "max": float(np.max(p99s)),
                                          "systems_over_1e-5": int(np.sum(np.asarray(p99s) > 1e-5))},
             "launches_per_evaluation": int(st["kernel_launches"]),
