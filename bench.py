@@ -41,6 +41,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The slowest replica's time: every rank passes its own total, all take
+    the same collective steps (an all-reduce with MAX, then a barrier). With
+    one rank it is the rank's own time."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def replicas_value(units_per_rank: float, steps: int, max_total_ms: float, world: int) -> float:
+    """Whole-job throughput of `world` replicas: the units all ranks processed
+    over the slowest rank's time."""
+    return world * units_per_rank * steps / (max_total_ms * 1e-3)
+
+
 CONFIGS = {
     "c1": dict(gen="plummer_ic", n=16384, p=8, theta=0.5, softening=1e-3, n_leaf=64,
                workload="Plummer N=16384 (r<=20, DF velocities), softening 1e-3, p=8, theta=0.5, leaf 64"),
@@ -318,14 +339,7 @@ def measure_eval(args, cfg, precision, mass, pos, dev, world, clk_sampler=None):
             m2l_ms.append(st["ms_m2l"])
             p2p_ms.append(st["ms_p2p"])
     torch.cuda.synchronize()
-    total_ms = sum(times)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(times), world, f"cuda:{dev}")
 
     # end to end through the host API: pinned host inputs in, host results out
     h_pos = torch.from_numpy(pos).pin_memory()
@@ -345,7 +359,7 @@ def measure_eval(args, cfg, precision, mass, pos, dev, world, clk_sampler=None):
         assert st_b == 0 and st_e == 0, fx.lib().fmmx_last_error(g._h)
         if i >= args.warmup:
             e2e_times.append(e0.elapsed_time(e1))
-    e2e_ms = sum(e2e_times) / len(e2e_times)
+    e2e_ms = max_over_ranks(sum(e2e_times) / len(e2e_times), world, f"cuda:{dev}")
 
     # accuracy against the FP64 direct sum on 4096 seeded targets
     rng = np.random.default_rng(4096)
@@ -431,7 +445,7 @@ def run_gpu(args, cfg, rank, world, local_rank):
         other = measure_eval(args, cfg, other_prec, mass, pos, dev, world)
     if rank != 0:
         return
-    value = world * n * args.steps / (main["total_ms"] * 1e-3)
+    value = replicas_value(n, args.steps, main["total_ms"], world)
     st = main["st"]
     rel = main["rel"]
     cpu = None
@@ -460,7 +474,7 @@ def run_gpu(args, cfg, rank, world, local_rank):
     }
     if other is not None:
         orel = other["rel"]
-        ov = world * n * args.steps / (other["total_ms"] * 1e-3)
+        ov = replicas_value(n, args.steps, other["total_ms"], world)
         line["compare"] = {"precision": "plain" if args.precision == "mixed" else "mixed", "value": ov,
                            "ms_per_step": other["total_ms"] / args.steps,
                            "force_err_p50": float(np.percentile(orel, 50)),
@@ -533,14 +547,7 @@ def measure_kdk(args, cfg, precision, mass, pos, vel, tg, dev, world, clk_sample
             st = g.stats()
             errs.append(force_err())
     torch.cuda.synchronize()
-    total_ms = sum(times)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([total_ms], dtype=torch.float64, device=cuda)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(times), world, cuda)
     g.close()
 
     # end to end: the reference's loop through the host API
@@ -590,7 +597,8 @@ def measure_kdk(args, cfg, precision, mass, pos, vel, tg, dev, world, clk_sample
     solo.close()
     p99s = [float(np.percentile(e, 99)) for e in errs]
     p50s = [float(np.percentile(e, 50)) for e in errs]
-    return dict(times=times, total_ms=total_ms, st=st, e2e_ms=float(np.mean(e2e_times)), p99s=p99s, p50s=p50s,
+    e2e_ms = max_over_ranks(float(np.mean(e2e_times)), world, cuda)
+    return dict(times=times, total_ms=total_ms, st=st, e2e_ms=e2e_ms, p99s=p99s, p50s=p50s,
                 m2l_ms=float(np.mean(m2l_solo)), p2p_ms=float(np.mean(p2p_solo)), m2l_ms_in_step=st["ms_m2l"],
                 ntargets=len(tg), solo_st=sst)
 
@@ -613,7 +621,7 @@ def run_headline(args, cfg, rank, world, local_rank):
         other = measure_kdk(args, cfg, other_prec, mass, pos, vel, tg, dev, world)
     if rank != 0:
         return
-    value = world * n * args.steps / (main["total_ms"] * 1e-3)
+    value = replicas_value(n, args.steps, main["total_ms"], world)
     st = main["st"]
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -643,7 +651,7 @@ def run_headline(args, cfg, rank, world, local_rank):
         "roofline": roofline(args, cfg, main, args.precision, dev), "cpu_baseline": cpu, "clocks": clk.summary(),
     }
     if other is not None:
-        ov = world * n * args.steps / (other["total_ms"] * 1e-3)
+        ov = replicas_value(n, args.steps, other["total_ms"], world)
         line["compare"] = {"precision": "plain" if args.precision == "mixed" else "mixed", "value": ov,
                            "ms_per_step": other["total_ms"] / args.steps,
                            "force_err_p50": float(np.median(other["p50s"])),

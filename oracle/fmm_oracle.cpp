@@ -16,8 +16,8 @@
 // the reference cannot be run here. The restatement is pinned against every
 // known-answer test the reference's own test suite holds and against the
 // end-to-end outputs the reference publishes (the N = 1e4 exit-gate errors,
-// todo.md:586; the N = 1e6 walk statistics, PERF-ANALYSIS.md:50-52), all in
-// tests/test_oracle.py.
+// todo.md:586; the N = 1e6 walk statistics, PERF-ANALYSIS.md:50-52; kept in
+// tests/golden/reference_published.json), all in tests/test_oracle.py.
 //
 // Extensions beyond the reference (flagged in every entry point): Plummer
 // softening in P2P and the direct sum, a geometric opening-angle MAC, a
