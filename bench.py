@@ -963,7 +963,8 @@ def run_serve(args, cfg, rank, world, local_rank):
         sessions.append(Session(sid=i, mass=m, pos=p, vel=v, steps=args.serve_steps, dt=1e-3, arrival=float(t)))
     kw = dict(p=cfg["p"], theta=cfg["theta"], softening=cfg["softening"], n_leaf=cfg["n_leaf"],
               precision=args.precision, budget_bytes=args.budget_gb * 1e9, refresh_every=args.refresh_every)
-    srv = Server(**kw, latency_slo=args.latency_slo)  # calibrates the isolated step time first
+    srv = Server(**kw, latency_slo=args.latency_slo,  # calibrates the isolated step time first
+                 headroom=args.headroom if args.headroom > 0 else None)
     srv.start()  # every lane on its own thread and stream
     t0 = time.perf_counter()
     k = 0
@@ -1052,6 +1053,8 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=160.0)
     ap.add_argument("--isolated-samples", type=int, default=10)
     ap.add_argument("--latency-slo", type=float, default=2.0)
+    ap.add_argument("--headroom", type=float, default=0.0,
+                    help="c5: admission bound as a multiple of isolated latency (0: 0.8 x latency-slo)")
     ap.add_argument("--m2l", default="auto", choices=["auto", "naive", "rotation"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--ref-budget-s", type=float, default=150.0,
