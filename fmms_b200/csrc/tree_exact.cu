@@ -961,7 +961,7 @@ __device__ __forceinline__ int warp_append(int* counter, bool mine, int lane) {
 // need -- both cells' leaf flags, geometry and children -- is issued at once
 // after the entry, and the three appends (M2L, P2P, next frontier) are one
 // atomic instruction from three lanes.
-__global__ void __launch_bounds__(256, 4) k_walk_iter(CellsView cv, MacParams mp, const double* __restrict__ pows,
+__global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict__ pows,
                             const double* __restrict__ fminv, WalkBufs w, int cur) {
     // After an overflow the frontier holds unwritten entries: stop, the host
     // retries with larger buffers.
