@@ -222,6 +222,7 @@ struct fmmx_ctx {
     DBuf<uint32_t> list_cnt2, long_bounds2;
     // near-field work units of the mixed P2P (per leaf: units, scratch bodies)
     DBuf<uint32_t> p2p_units, p2p_scr, p2p_uoff, p2p_soff;
+    DBuf<uint32_t> p2p_units_s, p2p_units_b, p2p_uoff_s, p2p_uoff_b;  // small-leaf units apart
     DBuf<double4> p2p_part;
     DBuf<float4> body_loc;  // mixed near field: bodies relative to their leaf's centre, FP32, with the mass
     DBuf<unsigned> p2p_next;
@@ -737,14 +738,18 @@ fmmx_status build_list(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp
     if (units) {
         // near-field work units: per leaf ceil(sources / P2P_UNIT_SRC), and the
         // scratch for the partial sums of leaves with several units
-        for (DBuf<uint32_t>* b : {&ctx->p2p_units, &ctx->p2p_scr, &ctx->p2p_uoff, &ctx->p2p_soff})
+        for (DBuf<uint32_t>* b : {&ctx->p2p_units, &ctx->p2p_scr, &ctx->p2p_uoff, &ctx->p2p_soff, &ctx->p2p_units_s,
+                                   &ctx->p2p_units_b, &ctx->p2p_uoff_s, &ctx->p2p_uoff_b})
             CK(b->ensure(nc + 1), "alloc lists");
-        CK(ctx->p2p_next.ensure(1), "alloc lists");
+        CK(ctx->p2p_next.ensure(2), "alloc lists");
         const DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
-        launch_p2p_plan(grid_for(nc + 1, 256), s, nc, lp, ctx->c_count.p, ctx->p2p_units.p, ctx->p2p_scr.p);
+        launch_p2p_plan(grid_for(nc + 1, 256), s, nc, lp, ctx->c_count.p, ctx->p2p_units.p, ctx->p2p_units_s.p,
+                        ctx->p2p_units_b.p, ctx->p2p_scr.p);
         CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_units.p, ctx->p2p_uoff.p, nc + 1, s), "p2p units");
+        CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_units_s.p, ctx->p2p_uoff_s.p, nc + 1, s), "p2p units");
+        CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_units_b.p, ctx->p2p_uoff_b.p, nc + 1, s), "p2p units");
         CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
-        LCOUNT(5);
+        LCOUNT(9);
     }
     // host read-back: the number of long segments (and the P2P scratch size)
     int nlong = 0;
@@ -774,8 +779,9 @@ fmmx_status near_mixed(fmmx_ctx* ctx, const DirList& lp, bool tm) {
     cudaEvent_t* ev = ctx->ev;
     if (tm) CK(cudaEventRecord(ev[12], s2), "event");
     const float soft2 = (float)(ctx->cfg.softening * ctx->cfg.softening);
-    CK(cudaMemsetAsync(ctx->p2p_next.p, 0, sizeof(unsigned), s2), "memset");
-    const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_soff.p, ctx->p2p_part.p, ctx->p2p_next.p};
+    CK(cudaMemsetAsync(ctx->p2p_next.p, 0, 2 * sizeof(unsigned), s2), "memset");
+    const P2pUnits units{ctx->p2p_uoff.p, ctx->p2p_uoff_s.p, ctx->p2p_uoff_b.p, ctx->p2p_soff.p, ctx->p2p_part.p,
+                         ctx->p2p_next.p};
     launch_p2p_mixed(ctx->cfg.p2p_tile > 0 ? ctx->cfg.p2p_tile : 512, ctx->nsm, s2, lp, nc, cv, units, n,
                      ctx->body_leaf.p, ctx->x.p, ctx->y.p, ctx->z.p, ctx->m.p, ctx->body_loc.p, soft2, ctx->nax.p,
                      ctx->nay.p, ctx->naz.p, ctx->npot.p);
@@ -806,7 +812,7 @@ fmmx_status far_mixed(fmmx_ctx* ctx, const DirList& lm, double* d_acc, double* d
         CK(launch_rotw_f32(p, lm, nc, cv, ctx->ellf.p, ctx->mom_f.p, ctx->loc_f.p, work, ctx->nsm, s), "m2l");
     }
     if (tm) CK(cudaEventRecord(ev[6], s), "event");
-    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 4);  // m2l, l2l per level, coords + p2p + combine, l2p
+    LCOUNT((ctx->n_m2l > 0 ? 1 : 0) + (ctx->nlevels - 1) + 5);  // m2l, l2l per level, coords + p2p (2) + combine, l2p
     for (int L = 1; L < ctx->nlevels; ++L) {
         const int cnt = ctx->lvl_count[L];
         const unsigned g = std::min<unsigned>(cnt, 16u * (unsigned)ctx->nsm);

@@ -157,15 +157,20 @@ __global__ void k_l2p_mixed(size_t n, const int32_t* body_leaf, const uint32_t* 
 // Near-field work units: the sources of a leaf in units of P2P_UNIT_SRC
 // source leaves (uoff: units of cell c at uoff[c] .. uoff[c+1]; soff: the
 // partial sums of a leaf with several units at part[soff[c] + k * count + i]).
+// The units of leaves of at most P2P_SMALL_NT bodies are numbered apart
+// (uoff_s) and run a warp each; the others (uoff_b) a block each.
 #define P2P_UNIT_SRC 1024
+#define P2P_SMALL_NT 32
 struct P2pUnits {
-    const uint32_t* uoff;  // ncells + 1
-    const uint32_t* soff;  // ncells + 1
+    const uint32_t* uoff;    // ncells + 1, all units
+    const uint32_t* uoff_s;  // ncells + 1, units of small leaves
+    const uint32_t* uoff_b;  // ncells + 1, units of the other leaves
+    const uint32_t* soff;    // ncells + 1
     double4* part;
-    unsigned* next;  // work counter, zero at launch
+    unsigned* next;  // two work counters (small, other), zero at launch
 };
 void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
-                     uint32_t* scratch);
+                     uint32_t* units_s, uint32_t* units_b, uint32_t* scratch);
 // loc: n float4 of scratch (bodies relative to their leaf's centre, with the mass)
 void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, CellsView cv, P2pUnits U, size_t n,
                       const int32_t* body_leaf, const double* x, const double* y, const double* z, const double* m,

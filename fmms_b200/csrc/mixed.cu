@@ -456,14 +456,19 @@ __device__ __forceinline__ void p2p_term(const float4 s, float xi, float yi, flo
 // k_p2p_combine adds per body in unit order (a fixed order: the results do
 // not depend on which block ran which unit).
 __global__ void k_p2p_plan(int ncells, DirList L, const uint32_t* __restrict__ count, uint32_t* __restrict__ units,
+                           uint32_t* __restrict__ units_s, uint32_t* __restrict__ units_b,
                            uint32_t* __restrict__ scratch) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += gridDim.x * blockDim.x) {
         uint32_t nu = 0;
+        bool small = false;
         if (c < ncells) {
             const uint32_t len = L.seg_end[c] - L.seg_begin[c];
             nu = (len + P2P_UNIT_SRC - 1) / P2P_UNIT_SRC;
+            small = count[c] <= P2P_SMALL_NT;
         }
         units[c] = nu;
+        units_s[c] = small ? nu : 0;
+        units_b[c] = small ? 0 : nu;
         scratch[c] = nu > 1 ? nu * count[c] : 0;
     }
 }
@@ -628,16 +633,16 @@ __global__ void __launch_bounds__(P2PM_BLOCK, 5) k_p2p_mixed(DirList L, int ncel
     __shared__ uint32_t unit_sh;
     const int tid = threadIdx.x;
     const int lane = tid & 31, wid = tid >> 5;
-    const uint32_t nunits = U.uoff[ncells];
+    const uint32_t nunits = U.uoff_b[ncells];
     const float2 soft2 = make_float2(soft2_1, soft2_1);
     for (;;) {
-        if (tid == 0) unit_sh = atomicAdd(U.next, 1u);
+        if (tid == 0) unit_sh = atomicAdd(U.next + 1, 1u);
         __syncthreads();
         const uint32_t u = unit_sh;
         __syncthreads();
         if (u >= nunits) break;
-        const int c = unit_cell(U.uoff, ncells, u);
-        const uint32_t k = u - U.uoff[c], nu = U.uoff[c + 1] - U.uoff[c];
+        const int c = unit_cell(U.uoff_b, ncells, u);
+        const uint32_t k = u - U.uoff_b[c], nu = U.uoff[c + 1] - U.uoff[c];
         const uint32_t beg = L.seg_begin[c] + k * P2P_UNIT_SRC;
         const uint32_t end = min(L.seg_end[c], beg + P2P_UNIT_SRC);
         const double cx = cv.cx[c], cy = cv.cy[c], cz = cv.cz[c];
@@ -814,6 +819,206 @@ __global__ void __launch_bounds__(P2PM_BLOCK, 5) k_p2p_mixed(DirList L, int ncel
     }
 }
 
+// Small target leaves (at most P2P_SMALL_NT bodies): a warp per work unit,
+// four independent warps per block, warp-synchronous (no block barriers).
+// With a few targets per leaf, a block per unit spends most of its
+// instructions on what every thread repeats per tile and per unit (the loop
+// setup, the barriers, the group reduction, finding the unit's leaf); a warp
+// pays them over a quarter of the threads. Same arithmetic as the block
+// kernel: two targets per lane, groups of G = ceil(nt / 2) lanes, R = 32 / G
+// groups over each tile's source pairs, packed FP32x2 interactions,
+// double-single sums, the leaf table for staging (chunks of at most
+// P2PW_CHUNK leaves and P2PW_MAP bodies), the target's own body masked.
+#define P2PW_TILE 128
+#define P2PW_CHUNK 128
+#define P2PW_MAP 2048
+#define P2PW_WARPS 4
+struct P2pWarpSmem {
+    float4 ta[P2PW_TILE / 2];
+    float4 tz[P2PW_TILE / 2];
+    float4 soff[P2PW_CHUNK];
+    uint32_t pre[P2PW_CHUNK + 1];
+    uint32_t sbase[P2PW_CHUNK];
+    float red[16][32];
+    uint8_t own[P2PW_MAP];
+};
+
+__global__ void __launch_bounds__(32 * P2PW_WARPS) k_p2p_mixed_small(DirList L, int ncells, CellsView cv, P2pUnits U,
+                                                                     const float4* __restrict__ loc, float soft2_1,
+                                                                     double* __restrict__ ax, double* __restrict__ ay,
+                                                                     double* __restrict__ az,
+                                                                     double* __restrict__ pot) {
+    __shared__ P2pWarpSmem smem_w[P2PW_WARPS];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    P2pWarpSmem& S = smem_w[threadIdx.x >> 5];
+    const uint32_t nunits = U.uoff_s[ncells];
+    const float2 soft2 = make_float2(soft2_1, soft2_1);
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(U.next, 1u);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= nunits) break;
+        const int c = unit_cell(U.uoff_s, ncells, u);
+        const uint32_t k = u - U.uoff_s[c], nu = U.uoff[c + 1] - U.uoff[c];
+        const uint32_t beg = L.seg_begin[c] + k * P2P_UNIT_SRC;
+        const uint32_t end = min(L.seg_end[c], beg + P2P_UNIT_SRC);
+        const double cx = cv.cx[c], cy = cv.cy[c], cz = cv.cz[c];
+        const uint32_t tf = cv.first[c];
+        const int nt = (int)cv.count[c];  // <= P2P_SMALL_NT (32) by the plan
+        const int G = (nt + 1) >> 1;
+        const int R = 32 / G;
+        const int g = lane % G, rep = lane / G;
+        const bool active = rep < R;
+        const int i0 = g, i1 = g + G;
+        const bool has1 = active && i1 < nt;
+        float x0 = 0, y0 = 0, z0 = 0, x1 = 0, y1 = 0, z1 = 0;
+        if (active) {
+            const float4 v = loc[tf + i0];
+            x0 = v.x; y0 = v.y; z0 = v.z;
+        }
+        if (has1) {
+            const float4 v = loc[tf + i1];
+            x1 = v.x; y1 = v.y; z1 = v.z;
+        }
+        const float2 nx0 = make_float2(-x0, -x0), ny0 = make_float2(-y0, -y0), nz0 = make_float2(-z0, -z0);
+        const float2 nx1 = make_float2(-x1, -x1), ny1 = make_float2(-y1, -y1), nz1 = make_float2(-z1, -z1);
+        DS a0x{0, 0}, a0y{0, 0}, a0z{0, 0}, p0{0, 0}, a1x{0, 0}, a1y{0, 0}, a1z{0, 0}, p1{0, 0};
+        float2 q0x{0, 0}, q0y{0, 0}, q0z{0, 0}, q0p{0, 0}, q1x{0, 0}, q1y{0, 0}, q1z{0, 0}, q1p{0, 0};
+        int held = 0;
+        auto flush = [&]() {
+            ds_add(a0x, q0x.x + q0x.y);
+            ds_add(a0y, q0y.x + q0y.y);
+            ds_add(a0z, q0z.x + q0z.y);
+            ds_add(p0, q0p.x + q0p.y);
+            ds_add(a1x, q1x.x + q1x.y);
+            ds_add(a1y, q1y.x + q1y.y);
+            ds_add(a1z, q1z.x + q1z.y);
+            ds_add(p1, q1p.x + q1p.y);
+            q0x = q0y = q0z = q0p = q1x = q1y = q1z = q1p = make_float2(0.f, 0.f);
+            held = 0;
+        };
+        for (uint32_t sc = beg; sc < end;) {
+            const int ns = (int)min((uint32_t)P2PW_CHUNK, end - sc);
+            __syncwarp();
+            // exclusive prefix of the chunk's source leaf sizes (one warp scan
+            // per 32 leaves, carried over); each lane remembers where the
+            // target leaf itself lies, if it holds it
+            uint32_t base = 0;
+            int self_q = P2PW_CHUNK, self_at = -1;
+            for (int q0 = 0; q0 < ns; q0 += 32) {
+                const int q = q0 + lane;
+                uint32_t v = 0;
+                int src = -1;
+                if (q < ns) {
+                    src = (int)L.src(L.key(sc + q));
+                    v = cv.count[src];
+                    S.soff[q] = make_float4((float)(cv.cx[src] - cx), (float)(cv.cy[src] - cy),
+                                            (float)(cv.cz[src] - cz), 0.f);
+                }
+                uint32_t incl = v;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (q < ns) {
+                    const uint32_t excl = base + incl - v;
+                    S.pre[q + 1] = excl + v;
+                    S.sbase[q] = cv.first[src] - excl;
+                    if (src == c) {
+                        self_q = q;
+                        self_at = (int)excl;
+                    }
+                }
+                base += __shfl_sync(FULL, incl, 31);
+            }
+            if (lane == 0) S.pre[0] = 0;
+            __syncwarp();
+            // the leaves whose bodies fit in the table (at least one)
+            unsigned fit = 0;
+            for (int q = lane; q < ns; q += 32) fit += S.pre[q + 1] <= P2PW_MAP ? 1u : 0u;
+            const int nl = max(1, (int)__reduce_add_sync(FULL, fit));
+            const bool mapped = S.pre[nl] <= P2PW_MAP;
+            const int sp = __reduce_max_sync(FULL, self_q < nl ? self_at : -1);
+            if (mapped)
+                for (int q = lane; q < nl; q += 32)
+                    for (uint32_t e = S.pre[q]; e < S.pre[q + 1]; ++e) S.own[e] = (uint8_t)q;
+            __syncwarp();
+            const uint32_t total = S.pre[nl];
+            sc += nl;
+            for (uint32_t b0 = 0; b0 < total; b0 += P2PW_TILE) {
+                const uint32_t nb = min((uint32_t)P2PW_TILE, total - b0);
+                const int npair = (int)(nb + 1) >> 1;
+                for (int q = lane; q < npair; q += 32) {
+                    float4 s2[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t gg = b0 + 2u * (uint32_t)q + (uint32_t)h;
+                        if (gg < b0 + nb) {
+                            const int l = mapped ? (int)S.own[gg] : 0;
+                            const float4 v = loc[gg + S.sbase[l]];
+                            const float4 o = S.soff[l];
+                            s2[h] = make_float4(v.x + o.x, v.y + o.y, v.z + o.z, v.w);
+                        } else {
+                            s2[h] = make_float4(1e18f, 0.f, 0.f, 0.f);  // massless padding
+                        }
+                    }
+                    S.ta[q] = make_float4(s2[0].x, s2[1].x, s2[0].y, s2[1].y);
+                    S.tz[q] = make_float4(s2[0].z, s2[1].z, s2[0].w, s2[1].w);
+                }
+                __syncwarp();
+                if (active) {
+                    const bool overlaps = sp >= 0 && (uint32_t)sp < b0 + nb && (uint32_t)sp + (uint32_t)nt > b0;
+                    if (!overlaps) {
+#pragma unroll 2
+                        for (int j = rep; j < npair; j += R) {
+                            const float4 a = S.ta[j], b = S.tz[j];
+                            p2p_pair(a, b, nx0, ny0, nz0, soft2, q0x, q0y, q0z, q0p);
+                            p2p_pair(a, b, nx1, ny1, nz1, soft2, q1x, q1y, q1z, q1p);
+                        }
+                    } else {
+                        // the target's own body sits at position sp + i in the sources
+                        const int s0 = sp + i0 - (int)b0, s1 = sp + i1 - (int)b0;
+                        for (int j = rep; j < npair; j += R) {
+                            const float4 a = S.ta[j], b = S.tz[j];
+                            float4 a0 = a, b0v = b, a1 = a, b1v = b;
+                            if (s0 >= 0 && j == (s0 >> 1)) mask_self(a0, b0v, s0 & 1, x0, y0, z0);
+                            if (s1 >= 0 && j == (s1 >> 1)) mask_self(a1, b1v, s1 & 1, x1, y1, z1);
+                            p2p_pair(a0, b0v, nx0, ny0, nz0, soft2, q0x, q0y, q0z, q0p);
+                            p2p_pair(a1, b1v, nx1, ny1, nz1, soft2, q1x, q1y, q1z, q1p);
+                        }
+                    }
+                    held += (npair - rep + R - 1) / R;
+                    if (held >= P2PM_FLUSH) flush();
+                }
+                __syncwarp();
+            }
+        }
+        flush();
+        S.red[0][lane] = a0x.hi; S.red[1][lane] = a0x.lo; S.red[2][lane] = a0y.hi; S.red[3][lane] = a0y.lo;
+        S.red[4][lane] = a0z.hi; S.red[5][lane] = a0z.lo; S.red[6][lane] = p0.hi; S.red[7][lane] = p0.lo;
+        S.red[8][lane] = a1x.hi; S.red[9][lane] = a1x.lo; S.red[10][lane] = a1y.hi; S.red[11][lane] = a1y.lo;
+        S.red[12][lane] = a1z.hi; S.red[13][lane] = a1z.lo; S.red[14][lane] = p1.hi; S.red[15][lane] = p1.lo;
+        __syncwarp();
+        // outputs: nt targets x 4 components, each the sum over the R groups
+        // in group order
+        for (int o = lane; o < 4 * nt; o += 32) {
+            const int t = o >> 2, comp = o & 3;
+            const int gi = t % G, half = t / G;  // target t = gi + half * G
+            const int row = 8 * half + 2 * comp;
+            double v = 0.0;
+            for (int r = 0; r < R; ++r) v += (double)S.red[row][r * G + gi] + (double)S.red[row + 1][r * G + gi];
+            if (nu == 1) {
+                double* out = comp == 0 ? ax : comp == 1 ? ay : comp == 2 ? az : pot;
+                out[tf + t] = v;
+            } else {
+                reinterpret_cast<double*>(U.part + U.soff[c] + k * (uint32_t)nt + t)[comp] = v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // The bodies of the leaves with several units: the units' partial sums, in
 // unit order (one warp per leaf).
 __global__ void k_p2p_combine(int ncells, CellsView cv, P2pUnits U, double* __restrict__ ax, double* __restrict__ ay,
@@ -843,8 +1048,8 @@ __global__ void k_p2p_combine(int ncells, CellsView cv, P2pUnits U, double* __re
 }
 
 void launch_p2p_plan(unsigned grid, cudaStream_t s, int ncells, DirList L, const uint32_t* count, uint32_t* units,
-                     uint32_t* scratch) {
-    k_p2p_plan<<<grid, 256, 0, s>>>(ncells, L, count, units, scratch);
+                     uint32_t* units_s, uint32_t* units_b, uint32_t* scratch) {
+    k_p2p_plan<<<grid, 256, 0, s>>>(ncells, L, count, units, units_s, units_b, scratch);
 }
 
 template <int TILE>
@@ -865,6 +1070,14 @@ void launch_p2p_mixed(int tile, int nsm, cudaStream_t s, DirList L, int ncells, 
                       const int32_t* body_leaf, const double* x, const double* y, const double* z, const double* m,
                       float4* loc, float soft2, double* ax, double* ay, double* az, double* pot) {
     k_local_coords<<<grid_for(n, 256), 256, 0, s>>>(n, body_leaf, cv, x, y, z, m, loc);
+    {  // the small leaves' units, a warp each, persistent
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2p_mixed_small, 32 * P2PW_WARPS, 0) !=
+                cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        k_p2p_mixed_small<<<nsm * per_sm, 32 * P2PW_WARPS, 0, s>>>(L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
+    }
     if (tile <= 128) launch_tile<128>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
     else if (tile <= 256) launch_tile<256>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
     else if (tile <= 512) launch_tile<512>(nsm, s, L, ncells, cv, U, loc, soft2, ax, ay, az, pot);
