@@ -29,10 +29,8 @@ the step latency of the same session run alone. At start-up the server
 calibrates, for Plummer and uniform-cube systems of 1e3 .. 1e6 bodies, the
 isolated step latency and the extra latency of a second system of the same
 size in the same forest. A session is admitted only if the batch's latency
-predicted with it -- the batch's last measured step latency (for a batch
-starting in an empty lane, the isolated latency of the slower system type)
-plus the session's calibrated extra latency (the larger of the two system
-types) -- stays within
+predicted with it -- the batch's last measured step latency plus the session's
+calibrated extra latency (the larger of the two system types) -- stays within
 `headroom` times the isolated latency (the smaller of the two types) of the
 batch's smallest session, and only while the lane's recent steps stay within
 that bound (feedback against prediction error). A tick in which sessions join
@@ -279,24 +277,16 @@ def _u8(a):
 
 class LatencyModel:
     """Calibrated step latencies (ms) against N: `iso(n)` the isolated step
-    latency of the faster system type (the latency target is taken against
-    it), `iso_hi(n)` that of the slower type (a batch's prediction starts from
-    it: a session's type is not known), `extra(n)` the added latency of one
-    more system of n bodies in a forest. Log-log interpolation, extrapolated
-    with the end slope."""
+    latency, `extra(n)` the added latency of one more system of n bodies in a
+    forest. Log-log interpolation, extrapolated with the end slope."""
 
-    def __init__(self, ns, iso_ms, extra_ms, iso_hi_ms=None):
+    def __init__(self, ns, iso_ms, extra_ms):
         self.ns = [int(n) for n in ns]
         self.iso_ms = [float(v) for v in np.maximum.accumulate(np.asarray(iso_ms, dtype=np.float64))]
-        hi = iso_ms if iso_hi_ms is None else np.maximum(np.asarray(iso_hi_ms, dtype=np.float64), iso_ms)
-        self.iso_hi_ms = [float(v) for v in np.maximum.accumulate(np.asarray(hi, dtype=np.float64))]
         self.extra_ms = [max(float(v), 1e-3) for v in np.maximum.accumulate(np.asarray(extra_ms, dtype=np.float64))]
 
     def iso(self, n) -> float:
         return _interp_loglog(self.ns, self.iso_ms, n)
-
-    def iso_hi(self, n) -> float:
-        return _interp_loglog(self.ns, self.iso_hi_ms, n)
 
     def extra(self, n) -> float:
         return _interp_loglog(self.ns, self.extra_ms, n)
@@ -407,14 +397,14 @@ class Lane:
                 # every member's step
                 fits = False
             if fits and model is not None and nmin is not None:
-                pred = (tau if tau is not None else model.iso_hi(nmin)) + model.extra(s.n)
+                pred = (tau if tau is not None else model.iso(nmin)) + model.extra(s.n)
                 fits = pred * self.corr <= srv.headroom * model.iso(min(nmin, s.n))
             if fits and srv.reserve(s.bytes_needed()):
                 self.queue.remove(s)
                 s.admitted_at = now
                 new.append(s)
                 if model is not None:
-                    tau = model.iso_hi(s.n) if pred is None else pred
+                    tau = model.iso(s.n) if pred is None else pred
                 nmin = s.n if nmin is None else min(nmin, s.n)
                 continue
             if model is None or (s.submitted_at is not None and now - s.submitted_at > srv.max_bypass_s):
@@ -725,7 +715,7 @@ class Server:
     def calibrate(self, ns=CALIBRATION_N, steps=5) -> LatencyModel:
         """Isolated step latency and the extra latency of a second system of
         the same size, for Plummer and uniform-cube systems of each size."""
-        iso, iso_hi, extra = [], [], []
+        iso, extra = [], []
         for i, n in enumerate(ns):
             iso_t, ext_t = [], []
             for kind in ("plummer", "uniform"):
@@ -743,13 +733,12 @@ class Server:
                 iso_t.append(one)
                 ext_t.append(two - one)
             iso.append(min(iso_t))
-            iso_hi.append(max(iso_t))
             extra.append(max(ext_t))
         for ln in self.lanes:
             ln.tick_ms.clear()
             ln.trace.clear()
             ln.bodies_stepped = 0
-        return LatencyModel(ns, iso, extra, iso_hi)
+        return LatencyModel(ns, iso, extra)
 
     # -------------------------------------------------------------- memory
     def reserve(self, nbytes) -> bool:

@@ -24,13 +24,10 @@ def session(sid, n, submitted_at=0.0, staged=True):
 
 
 class LinearModel:
-    """iso(n) = 1 ms + n / 1e5 ms (both system types), extra(n) = n / 1e5 ms."""
+    """iso(n) = 1 ms + n / 1e5 ms, extra(n) = n / 1e5 ms."""
 
     def iso(self, n):
         return 1.0 + n / 1e5
-
-    def iso_hi(self, n):
-        return self.iso(n)
 
     def extra(self, n):
         return n / 1e5
@@ -221,18 +218,3 @@ def test_admission_no_joins_after_a_slow_step():
     assert Lane.admit(ln, now=0.0) == []
     member.slow_steps = 0
     assert len(Lane.admit(ln, now=0.0)) == 1
-
-
-def test_latency_model_types_and_fresh_batch_prediction():
-    """A batch starting in an empty lane is predicted from the slower system
-    type's isolated latency (a session's type is not known), while the bound
-    stays the faster type's."""
-    m = LatencyModel([1e3, 1e4], [1.0, 2.0], [0.1, 0.5], iso_hi_ms=[1.6, 2.5])
-    assert m.iso(1e3) == pytest.approx(1.0) and m.iso_hi(1e3) == pytest.approx(1.6)
-    head, other = session(0, 1000), session(1, 1000)
-    ln = fake_lane([head, other], model=m)
-    # 1.6 + 0.1 > 1.6 * 1.0: the second session no longer fits beside the head
-    assert Lane.admit(ln, now=0.0) == [head]
-    m2 = LatencyModel([1e3, 1e4], [1.0, 2.0], [0.1, 0.5])  # one type: iso_hi = iso
-    ln2 = fake_lane([session(2, 1000), session(3, 1000)], model=m2)
-    assert len(Lane.admit(ln2, now=0.0)) == 2  # 1.0 + 0.1 <= 1.6
