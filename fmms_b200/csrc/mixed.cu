@@ -13,6 +13,8 @@
 //   L2L: F^_c[n][m] = (l_c/l_p)^{n+1} sum_{k,l} conj(Υ_k^l((s_p - s_c)/l_p)) F^_p[n+k][m+l]
 //   L2P: Ψ_0^0 = (1/l) sum conj(Υ_k^l(r^)) F^_k^l,  Ψ_1^m = (1/l^2) sum conj(Υ_k^l(r^)) F^_{k+1}^{m+l}
 // (the unnormalised forms are moments.rs:30-90 and translate.rs:175-309).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -281,59 +283,170 @@ void launch_upward_mixed(bool fp64, unsigned grid, int warps, cudaStream_t s, co
     }
 }
 
-// L2L for the cells of one level (L >= 1), one CTA per cell; A as above.
+// Υ column m as ups_column computes it, stored in the full layout (entry
+// (n, m) at n(n+1) + m for |m| <= n), with v_{n,-m} = (-1)^m conj(v_{n,m}).
 template <typename A>
-__global__ void __launch_bounds__(128) k_l2l_mixed(const int32_t* __restrict__ level_cells, int lstart, int lcnt,
-                                                  CellsView cv, const int32_t* __restrict__ parent,
-                                                  const double* __restrict__ ell, int p, zf* __restrict__ loc) {
-    extern __shared__ unsigned char smem_raw[];
-    const int H = (p + 1) * (p + 2) / 2;
-    cplx<A>* u = reinterpret_cast<cplx<A>*>(smem_raw);
-    zf* fp = reinterpret_cast<zf*>(u + H);
-    const int tid = threadIdx.x;
-    for (int j = blockIdx.x; j < lcnt; j += gridDim.x) {
+__device__ __forceinline__ void ups_column_full(A x, A y, A z, A r2, int p, int m, cplx<A>* u) {
+    auto put = [&](int n, cplx<A> v) {
+        u[n * (n + 1) + m] = v;
+        if (m) u[n * (n + 1) - m] = (m & 1) ? mk<A>(-v.re, v.im) : mk<A>(v.re, -v.im);
+    };
+    cplx<A> d = mk<A>(A(1), A(0));
+    for (int j = 1; j <= m; ++j) d = zmul(zscale(mk<A>(x, y), (A)g_tab.inv2m[j]), d);
+    put(m, d);
+    cplx<A> u1 = d, u2 = mk<A>(A(0), A(0));
+    for (int n = m + 1; n <= p; ++n) {
+        const A a = (A)(2 * n - 1) * z;
+        const cplx<A> un = zscale(zsub(zscale(u1, a), zscale(u2, r2)), (A)g_tab.invc[n][m]);
+        put(n, un);
+        u2 = u1;
+        u1 = un;
+    }
+}
+
+// L2L for the cells of one level (L >= 1), one warp per cell; A as above.
+//
+// Output (n, m) of the child's locals is ratio^{n+1} sum_{k <= p-n, |l| <= k}
+// conj(Υ_{k,l}(r)) L_{n+k, m+l} of the parent: (p-n+1)^2 products, 121 for
+// the monopole and 1 for degree p at p = 10. A thread per output leaves most
+// lanes idle behind the low degrees, so the products of all outputs are laid
+// out as one list ("items": output by output, k then l) of
+// T = q (q+1)^2 (q+2) / 12 entries (q = p + 1; 1,716 at p = 10) and every lane
+// takes an equal contiguous run of it. An output that lies inside one lane's
+// run is finished there; one that crosses runs leaves a partial sum in each
+// (slot 0: the output the run starts in, slot 1: the one it ends in), added
+// afterwards, in lane order, by the lane holding its first product -- a fixed
+// order, so the result bits do not depend on scheduling. The list is built
+// by every block at its start (item: Υ index, parent index, output, and a
+// last-product flag); Υ and the parent's locals sit in shared memory in the
+// full layout (both signs of m), so a product is two loads and four FMAs.
+#define L2LB_WARPS 4
+
+__host__ __device__ constexpr int l2l_items(int p) {
+    return (p + 1) * (p + 2) * (p + 2) * (p + 3) / 12;
+}
+
+template <typename A>
+static size_t l2l_smem(int p) {
+    const int P1 = p + 1, H = P1 * (P1 + 1) / 2, F2 = P1 * P1;
+    return (size_t)L2LB_WARPS * (F2 + 64 + H) * sizeof(cplx<A>) + (size_t)L2LB_WARPS * F2 * sizeof(zf) +
+           (size_t)(H + 1 + l2l_items(p)) * sizeof(uint32_t);
+}
+
+template <typename A>
+__global__ void __launch_bounds__(L2LB_WARPS * 32) k_l2l_mixed(const int32_t* __restrict__ level_cells, int lstart,
+                                                              int lcnt, CellsView cv,
+                                                              const int32_t* __restrict__ parent,
+                                                              const double* __restrict__ ell, int p,
+                                                              zf* __restrict__ loc) {
+    extern __shared__ __align__(16) unsigned char lsm[];
+    const int P1 = p + 1, H = P1 * (P1 + 1) / 2, F2 = P1 * P1, T = l2l_items(p);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    cplx<A>* U = reinterpret_cast<cplx<A>*>(lsm) + wid * F2;                      // Υ(r), full layout
+    cplx<A>* Pp = reinterpret_cast<cplx<A>*>(lsm) + L2LB_WARPS * F2 + wid * 64;  // [lane][2] partials
+    cplx<A>* R = reinterpret_cast<cplx<A>*>(lsm) + L2LB_WARPS * (F2 + 64) + wid * H;  // sums per output
+    zf* F = reinterpret_cast<zf*>(reinterpret_cast<cplx<A>*>(lsm) + L2LB_WARPS * (F2 + 64 + H)) + wid * F2;
+    uint32_t* einfo = reinterpret_cast<uint32_t*>(reinterpret_cast<zf*>(reinterpret_cast<cplx<A>*>(lsm) +
+                                                                        L2LB_WARPS * (F2 + 64 + H)) +
+                                                  L2LB_WARPS * F2);  // first item | n << 16
+    uint32_t* items = einfo + H + 1;
+
+    for (int e = threadIdx.x; e < H; e += blockDim.x) {
+        int n, m;
+        split_h(e, n, m);
+        int s = 0;
+        for (int q = 0; q < n; ++q) s += (q + 1) * (p - q + 1) * (p - q + 1);
+        const int w = p - n + 1;
+        s += m * w * w;
+        einfo[e] = (uint32_t)s | ((uint32_t)n << 16);
+        for (int k = 0; k <= p - n; ++k)
+            for (int l = -k; l <= k; ++l, ++s)
+                items[s] = (uint32_t)(k * (k + 1) + l) | ((uint32_t)((n + k) * (n + k + 1) + m + l) << 9) |
+                           ((uint32_t)e << 18) | (k == p - n && l == k ? 0x80000000u : 0u);
+    }
+    if (threadIdx.x == 0) einfo[H] = (uint32_t)T;
+    __syncthreads();
+
+    const int W = ((T + 31) / 32) | 1;  // an odd stride keeps the lanes' item reads on distinct banks
+    const int r0 = min(T, lane * W), r1 = min(T, r0 + W);
+    for (int j = blockIdx.x * L2LB_WARPS + wid; j < lcnt; j += gridDim.x * L2LB_WARPS) {
         const int c = level_cells[lstart + j];
         const int par = parent[c];
         if (par < 0) continue;
         const double il = 1.0 / ell[par];
         const A rx = (A)((cv.cx[par] - cv.cx[c]) * il), ry = (A)((cv.cy[par] - cv.cy[c]) * il),
                 rz = (A)((cv.cz[par] - cv.cz[c]) * il);
-        if (tid <= p) ups_column<A>(rx, ry, rz, rx * rx + ry * ry + rz * rz, p, tid, u);
+        if (lane <= p) ups_column_full<A>(rx, ry, rz, rx * rx + ry * ry + rz * rz, p, lane, U);
         const zf* lp = loc + (size_t)par * half_stride(p);
-        for (int e = tid; e < H; e += blockDim.x) fp[e] = lp[e];
-        __syncthreads();
+        for (int e = lane; e < H; e += 32) {
+            const int n = (int)(einfo[e] >> 16), m = e - n * (n + 1) / 2;
+            const zf v = lp[e];
+            F[n * (n + 1) + m] = v;
+            if (m) F[n * (n + 1) - m] = (m & 1) ? mk<float>(-v.re, v.im) : mk<float>(v.re, -v.im);
+        }
+        __syncwarp();
+        A sr = 0, si = 0;
+        uint32_t it = 0;
+        for (int i = r0; i < r1; ++i) {
+            it = items[i];
+            const cplx<A> a = U[it & 511u];
+            const zf b = F[(it >> 9) & 511u];
+            sr += a.re * (A)b.re + a.im * (A)b.im;  // conj(a) * b
+            si += a.re * (A)b.im - a.im * (A)b.re;
+            if (it & 0x80000000u) {
+                const int e = (int)((it >> 18) & 255u);
+                if ((int)(einfo[e] & 0xffffu) >= r0) R[e] = mk<A>(sr, si);  // the whole output is in this run
+                else Pp[2 * lane] = mk<A>(sr, si);                          // it started in an earlier run
+                sr = 0;
+                si = 0;
+            }
+        }
+        if (r1 > r0 && !(it & 0x80000000u)) {  // the run ends inside an output
+            const int e = (int)((it >> 18) & 255u);
+            Pp[2 * lane + ((int)(einfo[e] & 0xffffu) <= r0 ? 0 : 1)] = mk<A>(sr, si);
+        }
+        __syncwarp();
+        if (r1 > r0) {
+            const int e = (int)((items[r1 - 1] >> 18) & 255u);
+            const int s0 = (int)(einfo[e] & 0xffffu), s1 = (int)(einfo[e + 1] & 0xffffu);
+            if (s0 >= r0 && s1 > r1) {  // an output that starts in this run and crosses into the next ones
+                cplx<A> acc = Pp[2 * lane + (s0 == r0 ? 0 : 1)];
+                for (int q = lane + 1; q * W < s1; ++q) {
+                    acc.re += Pp[2 * q].re;
+                    acc.im += Pp[2 * q].im;
+                }
+                R[e] = acc;
+            }
+        }
+        __syncwarp();
         const A ratio = (A)(ell[c] * il);
         zf* lc = loc + (size_t)c * half_stride(p);
-        for (int e = tid; e < H; e += blockDim.x) {
-            int n, m;
-            split_h(e, n, m);
-            A sr = 0, si = 0;
-            for (int k = 0; k <= p - n; ++k) {
-                for (int l = -k; l <= k; ++l) {
-                    const cplx<A> a = half_get<A>(u, k, l);
-                    const zf b = half_get<float>(fp, n + k, m + l);
-                    sr += a.re * (A)b.re + a.im * (A)b.im;  // conj(a) * b
-                    si += a.re * (A)b.im - a.im * (A)b.re;
-                }
-            }
+        for (int e = lane; e < H; e += 32) {
+            const int n = (int)(einfo[e] >> 16);
             A sc = ratio;
             for (int q = 0; q < n; ++q) sc *= ratio;
             const zf cur = lc[e];
-            lc[e] = mk<float>((float)((A)cur.re + sr * sc), (float)((A)cur.im + si * sc));
+            const cplx<A> v = R[e];
+            lc[e] = mk<float>((float)((A)cur.re + v.re * sc), (float)((A)cur.im + v.im * sc));
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
 void launch_l2l_mixed(bool fp64, unsigned grid, cudaStream_t s, const int32_t* level_cells, int lstart, int lcnt,
                       CellsView cv, const int32_t* parent, const double* ell, int p, zf* loc) {
-    const int H = (p + 1) * (p + 2) / 2;
-    if (fp64)
-        k_l2l_mixed<double><<<grid, 128, H * (sizeof(zd) + sizeof(zf)), s>>>(level_cells, lstart, lcnt, cv, parent,
-                                                                           ell, p, loc);
-    else
-        k_l2l_mixed<float><<<grid, 128, H * (sizeof(zf) + sizeof(zf)), s>>>(level_cells, lstart, lcnt, cv, parent,
-                                                                          ell, p, loc);
+    const unsigned blocks = std::max(1u, std::min(grid, (unsigned)((lcnt + L2LB_WARPS - 1) / L2LB_WARPS)));
+    if (fp64) {
+        const size_t sm = l2l_smem<double>(p);
+        if (sm > 48 * 1024)
+            cudaFuncSetAttribute(k_l2l_mixed<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_l2l_mixed<double><<<blocks, L2LB_WARPS * 32, sm, s>>>(level_cells, lstart, lcnt, cv, parent, ell, p, loc);
+    } else {
+        const size_t sm = l2l_smem<float>(p);
+        if (sm > 48 * 1024)
+            cudaFuncSetAttribute(k_l2l_mixed<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_l2l_mixed<float><<<blocks, L2LB_WARPS * 32, sm, s>>>(level_cells, lstart, lcnt, cv, parent, ell, p, loc);
+    }
 }
 
 // L2P at every body plus the near field, scattered to particle-id order.
