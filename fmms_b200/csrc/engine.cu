@@ -704,9 +704,12 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
 // a counting sort on the destination, segment sorts, and -- after a host
 // read-back of the number of long segments -- CUB's segmented sort of those.
 // The two kinds run on different streams with their own scratch (tmp, cnt,
-// bounds), so that the P2P can start while the M2L list is being built.
-fmmx_status build_list(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp, DBuf<uint32_t>& cnt,
-                       DBuf<uint32_t>& bounds) {
+// bounds). list_launch queues a list's kernels without waiting on the device;
+// list_finish reads back its long-segment count (waiting for that stream) and
+// sorts the long segments. Both lists are launched before either is finished,
+// so their builds -- bound by atomics and latency, not by the SMs' arithmetic
+// -- run side by side.
+fmmx_status list_launch(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp, DBuf<uint32_t>& cnt) {
     const int nc = ctx->nc;
     const int npairs = near ? ctx->n_p2p : ctx->n_m2l;
     const size_t ndir = near ? (npairs > 0 ? 2 * (size_t)npairs - (size_t)ctx->nleaves : 0)  // one entry per self pair
@@ -751,6 +754,18 @@ fmmx_status build_list(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp
         CK(scan_u32(tmp.p, tmp.cap, ctx->p2p_scr.p, ctx->p2p_soff.p, nc + 1, s), "p2p units");
         LCOUNT(9);
     }
+    return FMMX_OK;
+}
+
+fmmx_status list_finish(fmmx_ctx* ctx, bool near, cudaStream_t s, DBuf<char>& tmp, DBuf<uint32_t>& bounds) {
+    const int nc = ctx->nc;
+    const int npairs = near ? ctx->n_p2p : ctx->n_m2l;
+    const size_t ndir = near ? (npairs > 0 ? 2 * (size_t)npairs - (size_t)ctx->nleaves : 0) : 2 * (size_t)npairs;
+    DBuf<uint32_t>& off = near ? ctx->p2p_off : ctx->m2l_off;
+    DBuf<uint32_t>& src_u = near ? ctx->p2p_src_u : ctx->m2l_src_u;
+    DBuf<uint32_t>& src = near ? ctx->p2p_src : ctx->m2l_src;
+    DBuf<int>& longs = near ? ctx->p2p_longs : ctx->m2l_longs;
+    const bool units = near && ctx->cfg.precision == FMMX_MIXED;
     // host read-back: the number of long segments (and the P2P scratch size)
     int nlong = 0;
     uint32_t nscr = 0;
@@ -962,7 +977,13 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     if (tm) CK(cudaEventRecord(ev[4], s2), "event");
     if (!reuse) {
         CK(cudaEventRecord(ctx->fork[1], s2), "event");  // the walk's pairs are in place
-        fmmx_status st = build_list(ctx, true, s2, ctx->cub_tmp, ctx->list_cnt, ctx->long_bounds);
+        fmmx_status st = list_launch(ctx, true, s2, ctx->cub_tmp, ctx->list_cnt);
+        if (st != FMMX_OK) return st;
+        CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L list reads the walk's pairs
+        if (tm) CK(cudaEventRecord(ev[14], s), "event");
+        st = list_launch(ctx, false, s, ctx->cub_tmp2, ctx->list_cnt2);
+        if (st != FMMX_OK) return st;
+        st = list_finish(ctx, true, s2, ctx->cub_tmp, ctx->long_bounds);
         if (st != FMMX_OK) return st;
     }
     if (tm) CK(cudaEventRecord(ev[5], s2), "event");
@@ -970,9 +991,8 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
     // (each list's pointers are taken after its build, which may reallocate it)
     const DirList lp{nullptr, ctx->p2p_src.p, ctx->p2p_off.p, ctx->p2p_off.p + 1, 32};
     // The near field starts on the second stream as soon as its list is
-    // built; the far field's list is built on the first stream after it is
-    // queued (beside the plain form's P2P; the mixed form's persistent P2P
-    // fills every SM, so there the list kernels follow it).
+    // built; the far field's list, launched beside it, is finished on the
+    // first stream after the near field is queued.
     if (mixed) {
         fmmx_status ms = near_mixed(ctx, lp, tm);
         if (ms != FMMX_OK) return ms;
@@ -986,9 +1006,7 @@ fmmx_status evaluate_impl(fmmx_ctx* ctx, const double* d_pos, const double* d_ma
         CK(cudaEventRecord(ctx->fork[2], s2), "event");
     }
     if (!reuse) {
-        CK(cudaStreamWaitEvent(s, ctx->fork[1], 0), "join");  // the M2L list reads the walk's pairs
-        if (tm) CK(cudaEventRecord(ev[14], s), "event");
-        fmmx_status st = build_list(ctx, false, s, ctx->cub_tmp2, ctx->list_cnt2, ctx->long_bounds2);
+        fmmx_status st = list_finish(ctx, false, s, ctx->cub_tmp2, ctx->long_bounds2);
         if (st != FMMX_OK) return st;
         if (tm) CK(cudaEventRecord(ev[15], s), "event");
         ctx->lists_valid = true;
