@@ -229,6 +229,7 @@ struct fmmx_ctx {
 
     DBuf<int> work;  // persistent-kernel work counter
     int nsm = 148;
+    int walk_blocks[2] = {0, 0};  // resident blocks of k_walk_iter<theta, Dehnen> on the whole device
     uint64_t launches = 0, launches_build = 0;
 
     fmmx_stats st;
@@ -666,11 +667,17 @@ fmmx_status walk_impl(fmmx_ctx* ctx, cudaStream_t s) {
         int hc[WC_SIZE];
         bool done = false;
         const int max_iter = 8 * FMMX_NLEVELS + 16;
+        // One kernel per MAC, so the theta form carries none of the Dehnen
+        // estimate's registers (54 against 80: four resident blocks per SM
+        // instead of three), launched with exactly the resident blocks: the
+        // grid-stride loop then runs in one wave instead of a last, partly
+        // filled one.
+        const bool dehnen = mp.mode == FMMX_MAC_DEHNEN;
+        int& wb = ctx->walk_blocks[dehnen ? 1 : 0];
+        if (wb == 0) wb = walk_iter_blocks_per_sm(dehnen) * ctx->nsm;
         for (int it = 0; it < max_iter && !done;) {
             for (int b = 0; b < 6; ++b, ++it) {
-                // (measured: a 64-register form at four resident blocks per SM was
-                // slower, 11.3 -> 12.2 ms at the clustered N = 2^22 workload)
-                k_walk_iter<<<8u * (unsigned)ctx->nsm, 256, 0, s>>>(cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
+                launch_walk_iter(dehnen, (unsigned)wb, s, cv, mp, ctx->pows.p, ctx->fmin.p, w, cur);
                 LCOUNT(1);
                 CK(cudaMemsetAsync(ctx->wcounts.p + cur, 0, sizeof(int), s), "memset");
                 cur ^= 1;

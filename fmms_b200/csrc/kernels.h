@@ -98,7 +98,11 @@ __global__ void k_m2m_exact_block(const int32_t* level_cells, int lstart, int lc
                                   zd* moments, double* pows, const double* f, double* fmin);
 __global__ void k_fprepass(CellsView cells, const double* x, const double* y, const double* z, const double* m,
                            size_t n, const uint64_t* off, int nsys, const int32_t* roots, double* f, int* err);
-__global__ void k_walk_iter(CellsView cv, MacParams mp, const double* pows, const double* fmin, WalkBufs w, int cur);
+// one dual-walk iteration over frontier `cur` (k_walk_iter<DEHNEN>: Dehnen's error-estimate MAC, else
+// theta and soft_gap), 256-thread blocks; and its resident blocks per SM
+void launch_walk_iter(bool dehnen, unsigned grid, cudaStream_t s, CellsView cv, MacParams mp, const double* pows,
+                      const double* fmin, WalkBufs w, int cur);
+int walk_iter_blocks_per_sm(bool dehnen);
 __global__ void k_pack_geo(int nc, const double* cx, const double* cy, const double* cz, const double* rho,
                            double4* geo);
 

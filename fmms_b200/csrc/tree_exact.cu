@@ -961,6 +961,7 @@ __device__ __forceinline__ int warp_append(int* counter, bool mine, int lane) {
 // need -- both cells' leaf flags, geometry and children -- is issued at once
 // after the entry, and the three appends (M2L, P2P, next frontier) are one
 // atomic instruction from three lanes.
+template <bool DEHNEN>
 __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict__ pows,
                             const double* __restrict__ fminv, WalkBufs w, int cur) {
     // After an overflow the frontier holds unwritten entries: stop, the host
@@ -999,7 +1000,7 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
                 }
             } else {
                 bool acc;
-                if (mp.mode == FMMX_MAC_DEHNEN)
+                if (DEHNEN)
                     acc = accept_dehnen(cv, mp, pows, fminv, a, b, ga, gb) &&
                           accept_dehnen(cv, mp, pows, fminv, b, a, gb, ga) && gap_ok(mp, ga, gb);
                 else
@@ -1013,8 +1014,13 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
                     kind = WK_SPLIT;
                     split_a = lb || (!la && ga.w >= gb.w);
                     int nch = 0;
+                    // chb takes the children of the cell that splits (element by
+                    // element, so both arrays stay in registers)
 #pragma unroll
-                    for (int o = 0; o < 8; ++o) nch += (split_a ? cha[o] : chb[o]) >= 0;
+                    for (int o = 0; o < 8; ++o) {
+                        chb[o] = split_a ? cha[o] : chb[o];
+                        nch += chb[o] >= 0;
+                    }
                     npush = nch;
                 }
             }
@@ -1065,12 +1071,25 @@ __global__ void k_walk_iter(CellsView cv, MacParams mp, const double* __restrict
         } else if (kind == WK_SPLIT) {
 #pragma unroll
             for (int o = 0; o < 8; ++o) {
-                const int c = split_a ? cha[o] : chb[o];
+                const int c = chb[o];
                 if (c < 0) continue;
                 fout[pos++] = split_a ? make_uint2(c, b) : make_uint2(a, c);
             }
         }
     }
+}
+
+void launch_walk_iter(bool dehnen, unsigned grid, cudaStream_t s, CellsView cv, MacParams mp, const double* pows,
+                      const double* fmin, WalkBufs w, int cur) {
+    if (dehnen) k_walk_iter<true><<<grid, 256, 0, s>>>(cv, mp, pows, fmin, w, cur);
+    else k_walk_iter<false><<<grid, 256, 0, s>>>(cv, mp, pows, fmin, w, cur);
+}
+
+int walk_iter_blocks_per_sm(bool dehnen) {
+    int per_sm = 0;
+    const cudaError_t e = dehnen ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_iter<true>, 256, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_iter<false>, 256, 0);
+    return e == cudaSuccess && per_sm > 0 ? per_sm : 1;
 }
 
 }  // namespace fmmx
