@@ -12,6 +12,8 @@
 // are then its sources in ascending order, src[off[c] .. off[c+1]), whatever
 // order the walk's atomics appended the pairs in, which fixes the
 // accumulation order and so every result bit.
+#include <atomic>
+
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
 
@@ -291,8 +293,20 @@ cudaError_t build_directed_list(void* tmp, size_t tmp_bytes, const uint2* pairs,
     k_scatter_dst<<<grid, 256, 0, s>>>(pairs, np, off, cnt, src_unsorted);
     k_sort_segments<<<grid_for((size_t)ncells * 32, 256, 64u * g_nsm), 256, 0, s>>>(off, ncells, src_unsorted, src,
                                                                                    mid, nmid, big, nbig);
-    k_sort_segments_large<128, SEG_MID><<<12 * g_nsm, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src, mid,
-                                                                                          nmid);
+    // exactly the resident blocks, so the middle segments are spread over
+    // blocks that all run at once
+    static std::atomic<int> large_per_sm{0};
+    if (large_per_sm.load() == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sort_segments_large<128, SEG_MID>, 128,
+                                                          SEG_MID * sizeof(uint32_t)) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        large_per_sm.store(b);
+    }
+    const unsigned large_grid = (unsigned)(large_per_sm.load() * g_nsm);
+    k_sort_segments_large<128, SEG_MID><<<large_grid, 128, SEG_MID * sizeof(uint32_t), s>>>(off, src_unsorted, src,
+                                                                                          mid, nmid);
     return cudaGetLastError();
 }
 
